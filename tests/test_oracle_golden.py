@@ -1,0 +1,49 @@
+"""Pins the CPU oracle against the reference's own golden vectors: the five
+regression certificates (results/reference_certificates/*.txt, test.sh) under
+both --method values, the README answers, and the published mean off-integer
+errors of the default Barnes–Hut run (test.sh:4,14,24,34,45)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, GOLDEN, golden_bcc, golden_certificate
+from oracle import pyoracle
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_oracle_barneshut_matches_golden(name, golden_dir):
+    o = pyoracle.Oracle().load_bcc(golden_bcc(name, golden_dir))
+    text, mean_off, _ = o.certificate(direct=False)
+    assert text == golden_certificate(name)
+    published = json.load(open(os.path.join(GOLDEN, "manifest.json")))["published_mean_off_integer_bh"]
+    # test.sh prints 6 significant digits.
+    assert mean_off == pytest.approx(published[name], rel=1e-5)
+
+
+@pytest.mark.parametrize("name", ["knittubeinit", "knittubebroken", "blenderobj", "houdiniobj"])
+def test_oracle_directsum_matches_golden(name, golden_dir):
+    o = pyoracle.Oracle().load_bcc(golden_bcc(name, golden_dir))
+    text, mean_off, _ = o.certificate(direct=True)
+    assert text == golden_certificate(name)
+    assert mean_off < 1e-12
+
+
+def test_readme_answers():
+    # README.md:71-78 (glove -> "70") and :86-94 (knittubebroken -> 5,6,-2).
+    assert golden_certificate("glove") == "70\n"
+    assert golden_certificate("knittubebroken") == "39\n5,6,-2\n"
+
+
+@pytest.mark.parametrize("name", ["knittubebroken", "houdiniobj"])
+def test_committed_pair_sums_reproduce(name, golden_dir):
+    o = pyoracle.Oracle().load_bcc(golden_bcc(name, golden_dir)).prepare(True)
+    ref = np.load(os.path.join(GOLDEN, "pairs", name + ".npz"))
+    pairs = o.pairs()
+    assert np.array_equal(pairs, ref["pairs"])
+    off, _ = o.polylines()
+    assert np.array_equal(np.diff(off), ref["vertex_counts"])
+    method = pyoracle.DIRECT_ONE_ARCTAN if len(off) - 1 < 6 else pyoracle.DIRECT_FAST
+    lk, _, _, _ = o.eval_pairs(method, pairs)
+    np.testing.assert_allclose(lk, ref["lk_direct"], rtol=0, atol=1e-9)
