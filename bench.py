@@ -1,0 +1,334 @@
+"""Benchmark of the linking-number hot path on B200.
+
+One step = the certificate's linking-number stage over every potential loop
+pair of the workload: tree build + Barnes–Hut traversal (+ beta retry, margin
+check and FP64 recompute) with the discretized polylines already in HBM.
+Metric: certificate ms and segment-pair throughput, Gsegpair/s =
+sum over pairs of n_i * n_j (post-Discretize segment counts, the
+direct-sum-equivalent work) / step time; the same numerator for every method.
+
+Default workload: random closed polymer loops, 200 loops x 50,000 Gaussian
+steps (10M segments), centres uniform in a cube of side 400, quadrupole BH,
+beta = 2 — seeded synthetic data. N > 1 (torchrun): every rank runs its own
+seeded instance (weak scaling, no data-path collective); the time is the max
+over ranks.
+
+--impl reference times the reference's CPU algorithm (the oracle port, the
+reference itself cannot be built here) on the host cores with all threads,
+each step a seeded sample of the same workload's pairs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "certificate ms & Gsegpair/s (exact certs): mixed+learned BH vs plain FP64 GPU"
+UNIT = "Gsegpair/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# Algorithmic bytes per evaluated Barnes–Hut node pair: two FP32 node records
+# of the reference-minimal layout (c_M 3 + C_D 9 + C_Q 27 + centre 3 + radius
+# 1 + 3 norms = 46 values x 4 B = 184 B each).
+BH_BYTES_PER_NODE_PAIR = 2 * 184
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+def make_workload(name: str, seed: int):
+    from fastlinkingnumbers_b200 import Model, workloads as W
+    if name == "polymer":
+        off, xyz = W.polymer(seed=seed)
+        cfg = {"workload": "polymer loops: 200 x 50,000-step closed Gaussian walks (10M segments), cube 400",
+               "loops": 200, "steps_per_loop": 50000}
+    elif name == "chain_mail":
+        off, xyz = W.chain_mail(seed=seed)
+        cfg = {"workload": "chain-mail sheet: 100 x 100 rings, 48-gons (480k segments)", "loops": 10000}
+    elif name == "ring_chain":
+        off, xyz = W.ring_chain(seed=seed)
+        cfg = {"workload": "ring chain: 64 rings x 32 segments", "loops": 64}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
+    t0 = time.perf_counter()
+    poff, pxyz, pairs, rounds = m.Prepare(True)
+    cfg["host_prepare_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+    cfg["discretize_rounds"] = int(rounds)
+    cfg["segments_after_discretize"] = int(poff[-1])
+    cfg["pairs"] = int(len(pairs))
+    return poff, pxyz, pairs, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample_run(poff, pxyz, pairs, target_s: float, seed: int, nthreads: int):
+    """Times the oracle (the reference's CPU algorithm: loop-pair parallel,
+    serial depth-first Barnes–Hut with the beta retry) on a seeded sample of
+    pairs sized for about target_s seconds; returns (Gsegpair/s, info)."""
+    from oracle import pyoracle
+    o = pyoracle.Oracle().set_polylines(poff, pxyz)
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(pairs))
+    n = np.diff(poff).astype(np.float64)
+    done, t_total, work, k = 0, 0.0, 0.0, max(nthreads, 1)
+    while done < len(order):
+        sel = pairs[order[done:done + k]]
+        t0 = time.perf_counter()
+        o.eval_pairs(pyoracle.BARNES_HUT, sel, bh_parallel=False, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        t_total += dt
+        work += float(np.sum(n[sel[:, 0]] * n[sel[:, 1]]))
+        done += len(sel)
+        if t_total >= target_s:
+            break
+        k = int(max(nthreads, min(4 * k, len(sel) * max(1.0, (target_s - t_total) / max(dt, 1e-3)))))
+    return work / t_total / 1e9, {"pairs": done, "seconds": round(t_total, 2), "segment_pairs": work}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed)
+    from oracle import pyoracle
+    threads = pyoracle.max_threads()
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, info = cpu_sample_run(poff, pxyz, pairs, args.cpu_seconds, args.seed + 17, threads)
+        if s >= args.warmup:
+            vals.append((v, info))
+    v = float(np.mean([x[0] for x in vals]))
+    info = vals[-1][1]
+    sample = (f"{info['pairs']} seeded random pairs of {len(pairs)} ({info['segment_pairs']:.3g} "
+              f"segment pairs), Barnes-Hut beta 2 with retry, oracle port of the reference")
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * info["seconds"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": cfg,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from fastlinkingnumbers_b200 import Engine, _native as N
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank)
+    stream = torch.cuda.current_stream()
+    eng = Engine(local_rank, stream.cuda_stream)
+    prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
+                           bh_tree=args.bh_tree)
+    d_xyz = torch.from_numpy(pxyz).cuda()
+    d_off = torch.from_numpy(poff).cuda()
+    d_pairs = torch.from_numpy(pairs).cuda()
+    npairs = len(pairs)
+    d_lk = torch.zeros(npairs, dtype=torch.float64, device="cuda")
+    d_err = torch.zeros(npairs, dtype=torch.float64, device="cuda")
+    d_flags = torch.zeros(npairs, dtype=torch.int32, device="cuda")
+    n = np.diff(poff).astype(np.float64)
+    units = float(np.sum(n[pairs[:, 0]] * n[pairs[:, 1]]))
+
+    def step():
+        eng.linking_numbers_device(d_xyz.data_ptr(), d_off.data_ptr(), len(poff) - 1,
+                                   d_pairs.data_ptr(), npairs, d_lk.data_ptr(), d_err.data_ptr(),
+                                   d_flags.data_ptr(), method=args.method, params=prm)
+        return eng.stats()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    st = []
+    for _ in range(args.steps):
+        st.append(step())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    lk = d_lk.cpu().numpy()
+    flags = d_flags.cpu().numpy()
+    value = world * units / (ms * 1e-3) / 1e9
+
+    # End to end through the host-array entry point: H2D of the polylines and
+    # pairs, the whole stage, D2H of the per-pair results, every step.
+    h_xyz = torch.from_numpy(pxyz).pin_memory().numpy()
+    h_off = torch.from_numpy(poff).pin_memory().numpy()
+    h_pairs = torch.from_numpy(pairs).pin_memory().numpy()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        elk, _, _ = eng.linking_numbers(h_xyz, h_off, h_pairs, args.method, params=prm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert np.array_equal(np.round(elk), np.round(lk)), "host and device entry points disagree"
+
+    s_last = st[-1]
+    peaks, peak_kind = _peaks()
+    main_ms = float(np.mean([s["ms_main_kernel"] for s in st]))
+    node_pairs = float(np.mean([s["bh_far_evals"] + s["bh_leaf_evals"] for s in st]))
+    if args.method == "barneshut":
+        achieved = BH_BYTES_PER_NODE_PAIR * node_pairs / (main_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "bh_traverse", "achieved": achieved,
+                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "peak_source": peak_kind, "traffic": args.traffic_bytes,
+                "algorithmic_bytes_per_launch": BH_BYTES_PER_NODE_PAIR * node_pairs,
+                "node_pairs_per_step": node_pairs, "ms_per_launch": main_ms,
+                "note": "algorithmic bytes = 2 x 184 B FP32 node record per evaluated node pair"}
+    else:
+        roof = {"bound": "fp32-issue", "kernel": "direct_" + args.precision, "ms_per_launch": main_ms,
+                "segment_pairs_per_s": units / (main_ms * 1e-3)}
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": dict(cfg, method=args.method, precision=args.precision,
+                       tree="curve-order" if args.bh_tree == 0 else "reference kd-median",
+                       l2="inputs and per-step trees larger than L2 (no flush needed)",
+                       parallelism=f"replicas x{world}"),
+        "certificate_ms": ms,
+        "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(pxyz.nbytes + poff.nbytes + pairs.nbytes),
+                "d2h_bytes_per_step": int(npairs * (8 + 8 + 4))},
+        "gpu_launches": int(sum(s["kernel_launches"] for s in st)),
+        "roofline": roof,
+        "clocks": clk,
+        "stats": {"pairs": npairs, "segment_pairs": units, "beta_retried": s_last["beta_retried"],
+                  "fp64_recomputed": s_last["fp64_recomputed"], "tree_build_ms": s_last["ms_tree_build"],
+                  "far_evals": s_last["bh_far_evals"], "leaf_evals": s_last["bh_leaf_evals"],
+                  "nonzero_links": int(np.sum(np.round(lk) != 0)), "flags_recomputed": int(np.sum(flags & 1))},
+    }
+    if rank == 0 and world == 1 and args.direct_sample > 0:
+        # Plain FP64 GPU direct sum and the mixed direct sum on a seeded sample
+        # of pairs, extrapolated by segment pairs (the full FP64 direct sum of
+        # this workload takes minutes).
+        rng = np.random.default_rng(args.seed + 5)
+        sel = pairs[rng.permutation(npairs)[:args.direct_sample]]
+        w = float(np.sum(n[sel[:, 0]] * n[sel[:, 1]]))
+        out = {}
+        for prec, name in ((N.PREC_FP64, "fp64"), (N.PREC_MIXED, "mixed")):
+            eng.linking_numbers(pxyz, poff, sel, "directsum", precision=prec)
+            s = eng.stats()
+            out[name] = {"sample_pairs": int(len(sel)), "kernel_ms": s["ms_main_kernel"],
+                         "Gsegpair_per_s": w / (s["ms_main_kernel"] * 1e-3) / 1e9,
+                         "extrapolated_certificate_ms": s["ms_main_kernel"] * units / w}
+        result["direct_sum_sample"] = out
+        result["speedup_vs_fp64_direct"] = out["fp64"]["extrapolated_certificate_ms"] / ms
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        from oracle import pyoracle
+        thr = pyoracle.max_threads()
+        v, info = cpu_sample_run(poff, pxyz, pairs, args.cpu_seconds, args.seed + 17, thr)
+        result["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": thr, "kind": "port",
+            "sample": f"{info['pairs']} seeded random pairs ({info['segment_pairs']:.3g} segment "
+                      f"pairs) in {info['seconds']} s; oracle port of the reference's BH"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="polymer", choices=["polymer", "chain_mail", "ring_chain"])
+    ap.add_argument("--method", default="barneshut", choices=["barneshut", "directsum"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--bh-tree", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--direct-sample", type=int, default=64)
+    ap.add_argument("--traffic-bytes", type=float, default=None)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,255 @@
+"""Host-side mirror of the reference's public interface for the linking-number
+path, over the C ABI of libfln.so.
+
+Names follow the reference (antequ/fastlinkingnumbers): ``Model``
+(include/model.h:24-75), ``LinkingNumberCertificate``
+(include/linking_number_certificate.h:25-131) and the per-pair functions of
+src/compute_link.h:62-87. Errors raise ``FlnError`` (a RuntimeError) where the
+reference throws std::runtime_error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from ._native import FlnError, default_params
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+class Engine:
+    """One CUDA device and stream (fln_ctx). ``stream`` is an optional
+    cudaStream_t handle (e.g. ``torch.cuda.current_stream().cuda_stream``)."""
+
+    def __init__(self, device: int = 0, stream: int = 0):
+        self._L = N.load()
+        h = C.c_void_p()
+        N.check(self._L.fln_ctx_create(int(device), C.c_void_p(stream or None), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fln_ctx_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stats(self) -> dict:
+        s = N.Stats()
+        N.check(self._L.fln_ctx_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def linking_numbers(self, xyz, loop_offsets, pairs, method: str = "barneshut",
+                        params: Optional[N.Params] = None, **overrides):
+        """Real-valued linking numbers of closed polylines for each (i, j) pair.
+
+        xyz: (V, 3) float64 vertices; loop_offsets: (L + 1,) int64 CSR offsets;
+        pairs: (P, 2) int32. Returns (lk, err, flags) numpy arrays."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        off = np.ascontiguousarray(loop_offsets, dtype=np.int64)
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        prm = params if params is not None else default_params(**overrides)
+        n = len(pairs)
+        lk = np.zeros(n)
+        err = np.zeros(n)
+        flags = np.zeros(n, dtype=np.int32)
+        N.check(self._L.fln_linking_numbers(
+            self._h, _ptr(xyz), _ptr(off), len(off) - 1, _ptr(pairs), n,
+            N.METHOD_DIRECTSUM if method == "directsum" else _method(method), C.byref(prm),
+            _ptr(lk), _ptr(err), _ptr(flags)))
+        return lk, err, flags
+
+    def linking_numbers_device(self, d_xyz: int, d_offsets: int, nloops: int, d_pairs: int,
+                               npairs: int, d_lk: int, d_err: int = 0, d_flags: int = 0,
+                               method: str = "barneshut", params: Optional[N.Params] = None,
+                               **overrides):
+        """Same as linking_numbers with every array already in device memory
+        (raw device pointers, e.g. torch ``tensor.data_ptr()``)."""
+        prm = params if params is not None else default_params(**overrides)
+        N.check(self._L.fln_linking_numbers_device(
+            self._h, C.c_void_p(d_xyz), C.c_void_p(d_offsets), int(nloops), C.c_void_p(d_pairs),
+            int(npairs), _method(method), C.byref(prm), C.c_void_p(d_lk),
+            C.c_void_p(d_err or None), C.c_void_p(d_flags or None)))
+
+    def direct_pair(self, curve1, curve2, precision: int = N.PREC_FP64) -> float:
+        a = np.ascontiguousarray(curve1, dtype=np.float64).reshape(-1, 3)
+        b = np.ascontiguousarray(curve2, dtype=np.float64).reshape(-1, 3)
+        out = C.c_double()
+        N.check(self._L.fln_direct_pair(self._h, _ptr(a), len(a), _ptr(b), len(b), precision,
+                                        C.byref(out)))
+        return out.value
+
+
+def _method(m: str) -> int:
+    if m == "directsum":
+        return N.METHOD_DIRECTSUM
+    if m == "barneshut":
+        return N.METHOD_BARNESHUT
+    raise FlnError(1, f"Invalid method: '{m}'.")
+
+
+_default_engine: Optional[Engine] = None
+
+
+def default_engine() -> Engine:
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine(0)
+    return _default_engine
+
+
+def ComputeLinkingNumberDirectFast(curve1, curve2, parallel: bool = False) -> float:
+    """src/compute_link.h:86 — FP64 direct sum of two closed polylines ((n, 3) arrays)."""
+    return default_engine().direct_pair(curve1, curve2, N.PREC_FP64)
+
+
+def ComputeLinkingNumberDirectOneArctanPerPair(curve1, curve2, parallel: bool = False) -> float:
+    """src/compute_link.h:62 — same integral; the GPU kernel serves both forms."""
+    return default_engine().direct_pair(curve1, curve2, N.PREC_FP64)
+
+
+class Model:
+    """A collection of curves (include/model.h:24-75)."""
+
+    def __init__(self):
+        self._L = N.load()
+        h = C.c_void_p()
+        N.check(self._L.fln_model_create(C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.fln_model_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def ImportFromFile(self, filename: str):
+        N.check(self._L.fln_model_load_bcc(self._h, os.fsencode(filename)))
+        return self
+
+    def ExportToFile(self, filename: str):
+        N.check(self._L.fln_model_save_bcc(self._h, os.fsencode(filename)))
+
+    def SetCurves(self, seg_type: int, counts, xyz):
+        """counts[c] points per curve (negative = closed loop), xyz (P, 3)."""
+        counts = np.ascontiguousarray(counts, dtype=np.int32)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        N.check(self._L.fln_model_set_curves(self._h, int(seg_type), len(counts), _ptr(counts),
+                                             _ptr(xyz)))
+        return self
+
+    def GetCurves(self):
+        """Returns (seg_type, counts, xyz)."""
+        nc = self._L.fln_model_num_curves(self._h)
+        npnt = self._L.fln_model_num_points(self._h)
+        t = C.c_int32()
+        counts = np.zeros(nc, dtype=np.int32)
+        xyz = np.zeros((max(npnt, 1), 3))
+        N.check(self._L.fln_model_get_curves(self._h, C.byref(t), _ptr(counts), _ptr(xyz)))
+        return t.value, counts, xyz[:npnt]
+
+    def num_curves(self) -> int:
+        return self._L.fln_model_num_curves(self._h)
+
+    def Prepare(self, discretize: bool = True):
+        """PLS -> Discretize -> PLS. Returns (loop_offsets, xyz, pairs, rounds)."""
+        r = C.c_int32()
+        N.check(self._L.fln_model_prepare(self._h, int(discretize), C.byref(r)))
+        nv, npairs = C.c_int64(), C.c_int64()
+        N.check(self._L.fln_model_prepared_sizes(self._h, C.byref(nv), C.byref(npairs)))
+        off = np.zeros(self.num_curves() + 1, dtype=np.int64)
+        xyz = np.zeros((max(nv.value, 1), 3))
+        pairs = np.zeros((max(npairs.value, 1), 2), dtype=np.int32)
+        N.check(self._L.fln_model_get_prepared(self._h, _ptr(off), _ptr(xyz), _ptr(pairs)))
+        return off, xyz[:nv.value], pairs[:npairs.value], r.value
+
+
+class LinkingNumberCertificate:
+    """include/linking_number_certificate.h:25-131."""
+
+    def __init__(self, filename: Optional[str] = None):
+        self._L = N.load()
+        self._h = None
+        if filename is not None:
+            self.ImportFromFile(filename)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.fln_certificate_destroy(self._h)
+            self._h = None
+
+    def _replace(self, h):
+        if self._h:
+            self._L.fln_certificate_destroy(self._h)
+        self._h = h
+
+    def ComputeFromModel(self, model: Model, force_direct_sum: bool = False,
+                         discretize: bool = True, barnes_hut_init_beta: float = 2.0,
+                         barnes_hut_beta_limit: float = 10.0, engine: Optional[Engine] = None,
+                         **overrides):
+        eng = engine or default_engine()
+        prm = default_params(barnes_hut_init_beta=barnes_hut_init_beta,
+                             barnes_hut_beta_limit=barnes_hut_beta_limit, **overrides)
+        h = C.c_void_p()
+        N.check(self._L.fln_certificate_compute(eng.handle, model.handle, int(force_direct_sum),
+                                                int(discretize), C.byref(prm), C.byref(h)))
+        self._replace(h)
+        return self
+
+    def ImportFromFile(self, filename: str):
+        h = C.c_void_p()
+        N.check(self._L.fln_certificate_load(os.fsencode(filename), C.byref(h)))
+        self._replace(h)
+        return self
+
+    def ExportToFile(self, filename: str):
+        N.check(self._L.fln_certificate_save(self._h, os.fsencode(filename)))
+
+    def text(self) -> str:
+        n = self._L.fln_certificate_text(self._h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        self._L.fln_certificate_text(self._h, buf, n + 1)
+        return buf.value.decode()
+
+    def entries(self) -> np.ndarray:
+        n = self._L.fln_certificate_num_entries(self._h)
+        out = np.zeros((max(n, 1), 3), dtype=np.int32)
+        N.check(self._L.fln_certificate_entries(self._h, _ptr(out)))
+        return out[:n]
+
+    def pairs(self):
+        """Per evaluated pair: (pairs (P, 2), lk, err, flags)."""
+        n = self._L.fln_certificate_num_pairs(self._h)
+        pr = np.zeros((max(n, 1), 2), dtype=np.int32)
+        lk, err = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        fl = np.zeros(max(n, 1), dtype=np.int32)
+        N.check(self._L.fln_certificate_pairs(self._h, _ptr(pr), _ptr(lk), _ptr(err), _ptr(fl)))
+        return pr[:n], lk[:n], err[:n], fl[:n]
+
+    def ExportDiffsToFiles(self, out_diff_links_filename: str, out_diff_curves_filename: str,
+                           other: "LinkingNumberCertificate"):
+        N.check(self._L.fln_certificate_export_diffs(
+            self._h, other._h, os.fsencode(out_diff_links_filename),
+            os.fsencode(out_diff_curves_filename)))
+
+    def Equals(self, other: "LinkingNumberCertificate") -> bool:
+        return bool(self._L.fln_certificate_equals(self._h, other._h))
+
+    def __eq__(self, other):
+        return self.Equals(other)
+
+    def __ne__(self, other):
+        return not self.Equals(other)

@@ -1,0 +1,826 @@
+// Two-tree Barnes–Hut linking numbers on B200 (sm_100a).
+//
+// Trees. One binary tree per loop over its segments, leaves = single
+// segments. Default ("curve-order"): node = contiguous segment range
+// [lo, hi), split at lo + (hi - lo) / 2; a polyline is continuous, so these
+// ranges are spatially compact and the tree needs no sort. Its topology is
+// implicit: the internal node splitting at s has local id s - 1, found by a
+// root-to-node descent per node. Optionally the reference's kd-median tree
+// (ModifiedKdBVH.h:207-237) is built on the host and uploaded (bh_tree = 1).
+// Local ids: internal nodes 0..n-2, leaf of object position p = n-1+p.
+//
+// Moments (compute_link.h:95-114, compute_link.cpp:333-389) are built in
+// FP64 bottom-up: each leaf thread walks to the root; at every parent the
+// second arriving child computes the parent (box union, centre, the Eq. 21-23
+// shift of monopole c_M, dipole C_D, quadrupole C_Q) and continues. They are
+// then stored for traversal in FP32 relative to the node centre; the centre
+// itself stays FP64 so node separations are formed in FP64. Each C_Q[k] is
+// symmetric in its last two indices (leaf c_k c c^T / 12; the shift adds
+// c_k r r^T + (r D_k) + (r D_k)^T), so 6 of its 9 entries are stored.
+//
+// Traversal (compute_link.cpp:547-666, :695-841). One warp per loop pair,
+// pairs taken from a device queue. The warp keeps a LIFO of node pairs in
+// shared memory (spilling its oldest half to a global buffer when full) and
+// classifies up to 32 pairs per step, one per lane:
+//   leaf-leaf        -> exact one-arctan term (compute_link.cpp:576-606);
+//   far (|dr|^2 + eps^2 > (r1 + r2)^2 beta^2 + eps^2)
+//                    -> monopole + dipole + quadrupole (Eq. 29-30) and the
+//                       Eq. 14 error estimate (compute_link.cpp:411-524);
+//   otherwise        -> push the two children of the larger node (the
+//                       internal one if the other is a leaf).
+// Far and leaf pairs go to two per-warp queues and are evaluated 32 at a
+// time, so the expensive branches run with full warps. Leaf-leaf pairs
+// closer than one segment length are evaluated in FP64 from the vertices.
+// Sums are FP64 per lane, reduced per pair in a fixed order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "engine.hpp"
+
+namespace fln {
+
+namespace {
+
+constexpr double kInvTwoPi = 0.15915494309189533576888376337251436;
+constexpr double kInvFourPi = 0.079577471545947667884441881686257181;
+constexpr double kInvRt3 = 0.57735026918962576450914878050195746;
+constexpr int kWarps = 4;          // warps per traversal CTA
+constexpr int kStack = 512;        // shared-memory stack entries per warp
+constexpr int kSpill = 8192;       // global spill entries per warp
+
+// FP64 build record.
+struct BuildNode {
+  double lo[3], hi[3];
+  double mid[3];
+  double t[3];
+  double D[9];   // row-major
+  double Q[18];  // Q_k symmetric: (xx, yy, zz, xy, xz, yz) for k = 0, 1, 2
+};
+
+// Traversal records.
+struct __align__(16) NodeHdr {
+  double m[3];      // centre (leaves: segment midpoint)
+  double r;         // half the box diagonal
+  double rsq;       // its square, 0.25 |diag|^2, for the reference's split rule
+  int32_t left;     // internal: local child ids; leaf: left = -1 - segment
+  int32_t right;
+};
+static_assert(sizeof(NodeHdr) == 48, "NodeHdr layout");
+struct __align__(16) NodeMom {
+  float t[3];
+  float D[9];
+  float Q[18];
+  float tn, dn, qn;
+  float pad[3];
+};
+static_assert(sizeof(NodeMom) == 144, "NodeMom layout");
+
+struct TreeArgs {
+  const double *xyz;
+  const int64_t *off;        // loop vertex offsets
+  const int64_t *node_base;  // loop -> first global node
+  const int32_t *loops;      // loops that need a tree
+  int32_t nloops;
+  int32_t *children;         // 2 per global node (internal nodes only used)
+  int32_t *parent;           // per global node
+  int32_t *leaf_seg;         // per global node: segment of a leaf (kd trees permute)
+  int32_t *arrive;           // per global node: arrival counter
+  BuildNode *bn;
+  NodeHdr *hdr;
+  NodeMom *mom;
+};
+
+__device__ __forceinline__ int find_loop_of(const int64_t *start, int n, int64_t x) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (start[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Curve-order topology: thread per internal node (local id s - 1 splits at s).
+// seg_start[k] = sum of (n - 1) over the first k listed loops.
+__global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t total_internal) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total_internal) return;
+  const int k = find_loop_of(seg_start, A.nloops, g);
+  const int l = A.loops[k];
+  const int64_t n = A.off[l + 1] - A.off[l];
+  const int32_t node = (int32_t)(g - seg_start[k]);  // local internal id
+  const int64_t s = node + 1;                        // split position
+  const int64_t base = A.node_base[l];
+  int64_t lo = 0, hi = n;
+  int32_t par = -1;
+  for (int depth = 0; depth < 64; ++depth) {
+    const int64_t m = lo + (hi - lo) / 2;
+    if (m == s) break;
+    par = (int32_t)(m - 1);
+    if (s < m) hi = m;
+    else lo = m;
+  }
+  const int32_t leaf0 = (int32_t)(n - 1);
+  const int32_t left = (s - lo == 1) ? leaf0 + (int32_t)lo : (int32_t)(lo + (s - lo) / 2 - 1);
+  const int32_t right = (hi - s == 1) ? leaf0 + (int32_t)s : (int32_t)(s + (hi - s) / 2 - 1);
+  A.children[2 * (base + node)] = left;
+  A.children[2 * (base + node) + 1] = right;
+  A.parent[base + node] = par;
+  A.parent[base + left] = node;
+  A.parent[base + right] = node;
+  A.arrive[base + node] = 0;
+}
+
+// Leaves of every listed loop: leaf_seg is identity for curve-order trees
+// (the host fills it for kd trees).
+__global__ void identity_leaves(TreeArgs A, const int64_t *seg_start2, int64_t total) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int k = find_loop_of(seg_start2, A.nloops, g);
+  const int l = A.loops[k];
+  const int64_t n = A.off[l + 1] - A.off[l];
+  const int64_t p = g - seg_start2[k];
+  A.leaf_seg[A.node_base[l] + n - 1 + p] = (int32_t)p;
+}
+
+// Reads a record written by another thread of this launch: L2 loads (the
+// writer fenced before its arrival count), never a stale L1 line.
+__device__ __forceinline__ void load_cg(const BuildNode *src, BuildNode &dst) {
+  const double *s = reinterpret_cast<const double *>(src);
+  double *d = reinterpret_cast<double *>(&dst);
+  for (int a = 0; a < (int)(sizeof(BuildNode) / sizeof(double)); ++a) d[a] = __ldcg(s + a);
+}
+
+// Shift child moments onto the parent centre (Eqs. 21-23 of Qu & James 2021,
+// as compute_link.cpp:367-381): c += c_c; D += D_c + c_c r^T;
+// Q_k += Q_c,k + r D_c,k^T-row terms + c_c,k r r^T, with r = m_c - m.
+__device__ void accumulate_child(BuildNode &P, const BuildNode &C) {
+  const double r[3] = {C.mid[0] - P.mid[0], C.mid[1] - P.mid[1], C.mid[2] - P.mid[2]};
+  for (int a = 0; a < 3; ++a) P.t[a] += C.t[a];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) P.D[3 * a + b] += C.D[3 * a + b] + C.t[a] * r[b];
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int k = 0; k < 3; ++k)
+    for (int e = 0; e < 6; ++e) {
+      const int i = ii[e], j = jj[e];
+      P.Q[6 * k + e] += C.Q[6 * k + e] + r[j] * C.D[3 * k + i] + r[i] * C.D[3 * k + j] + C.t[k] * (r[i] * r[j]);
+    }
+}
+
+__device__ void finish_record(const BuildNode &B, NodeHdr &H, NodeMom &M, bool leaf, int32_t seg, int32_t l,
+                              int32_t r) {
+  const double dx = B.hi[0] - B.lo[0], dy = B.hi[1] - B.lo[1], dz = B.hi[2] - B.lo[2];
+  H.m[0] = B.mid[0];
+  H.m[1] = B.mid[1];
+  H.m[2] = B.mid[2];
+  H.rsq = 0.25 * (dx * dx + dy * dy + dz * dz);
+  H.r = sqrt(H.rsq);
+  H.left = leaf ? -1 - seg : l;
+  H.right = leaf ? -1 : r;
+  const double tn = sqrt(B.t[0] * B.t[0] + B.t[1] * B.t[1] + B.t[2] * B.t[2]);
+  double dd = 0, qq = 0;
+  for (int a = 0; a < 9; ++a) dd += B.D[a] * B.D[a];
+  for (int k = 0; k < 3; ++k)
+    for (int e = 0; e < 6; ++e) qq += (e < 3 ? 1.0 : 2.0) * B.Q[6 * k + e] * B.Q[6 * k + e];
+  for (int a = 0; a < 3; ++a) M.t[a] = (float)B.t[a];
+  for (int a = 0; a < 9; ++a) M.D[a] = (float)B.D[a];
+  for (int a = 0; a < 18; ++a) M.Q[a] = (float)B.Q[a];
+  M.tn = (float)tn;
+  M.dn = (float)(sqrt(dd) * kInvRt3);
+  // Leaf: |c|^3 / 36, which is also (1/3) ||C_Q||_F for c c c^T / 12.
+  M.qn = (float)(leaf ? tn * tn * tn / 36.0 : sqrt(qq) / 3.0);
+  M.pad[0] = M.pad[1] = M.pad[2] = 0.f;
+}
+
+// Thread per leaf: initialise the leaf (compute_link.cpp:351-363) and walk
+// up; the second child to arrive at a parent builds it.
+__global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t total) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int k = find_loop_of(seg_start2, A.nloops, g);
+  const int l = A.loops[k];
+  const int64_t o = A.off[l], n = A.off[l + 1] - o;
+  const int64_t base = A.node_base[l];
+  int32_t node = (int32_t)(n - 1 + (g - seg_start2[k]));
+  const int32_t seg = A.leaf_seg[base + node];
+  {
+    BuildNode B;
+    const int64_t v0 = o + seg, v1 = o + (seg + 1 == n ? 0 : seg + 1);
+    double p0[3], p1[3];
+    for (int a = 0; a < 3; ++a) {
+      p0[a] = A.xyz[3 * v0 + a];
+      p1[a] = A.xyz[3 * v1 + a];
+      B.lo[a] = fmin(p0[a], p1[a]);
+      B.hi[a] = fmax(p0[a], p1[a]);
+      B.mid[a] = 0.5 * p0[a] + 0.5 * p1[a];
+      B.t[a] = p1[a] - p0[a];
+    }
+    for (int a = 0; a < 9; ++a) B.D[a] = 0.0;
+    const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+    for (int kk = 0; kk < 3; ++kk)
+      for (int e = 0; e < 6; ++e) B.Q[6 * kk + e] = ((1.0 / 12.0) * B.t[kk]) * (B.t[ii[e]] * B.t[jj[e]]);
+    A.bn[base + node] = B;
+    finish_record(B, A.hdr[base + node], A.mom[base + node], true, seg, 0, 0);
+  }
+  for (int guard = 0; guard < 128; ++guard) {
+    const int32_t par = A.parent[base + node];
+    if (par < 0) break;
+    __threadfence();
+    if (atomicAdd(&A.arrive[base + par], 1) == 0) break;  // first arrival stops
+    __threadfence();
+    const int32_t cl = A.children[2 * (base + par)], cr = A.children[2 * (base + par) + 1];
+    BuildNode L, R;
+    load_cg(A.bn + base + cl, L);
+    load_cg(A.bn + base + cr, R);
+    BuildNode P;
+    for (int a = 0; a < 3; ++a) {
+      P.lo[a] = fmin(L.lo[a], R.lo[a]);
+      P.hi[a] = fmax(L.hi[a], R.hi[a]);
+      P.mid[a] = 0.5 * (P.hi[a] + P.lo[a]);
+      P.t[a] = 0.0;
+    }
+    for (int a = 0; a < 9; ++a) P.D[a] = 0.0;
+    for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
+    accumulate_child(P, L);
+    accumulate_child(P, R);
+    A.bn[base + par] = P;
+    finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
+    node = par;
+  }
+}
+
+// ------------------------------------------------------------------ traversal
+struct TravArgs {
+  const double *xyz;
+  const int64_t *off;
+  const int64_t *node_base;
+  const NodeHdr *hdr;
+  const NodeMom *mom;
+  const int32_t *slot_loops;  // 2 per slot
+  const int32_t *slot_pair;   // slot -> caller pair index
+  const double *itolsq;       // per slot beta^2
+  int32_t nslots;
+  double epssq;
+  double *lk;                 // per caller pair
+  double *err;                // per caller pair (Eq. 14 sum, unscaled)
+  double *counts;             // [0] far evals, [1] leaf evals
+  int2 *spill;                // kSpill per warp
+  int32_t tree_kind;          // 0 curve-order (root n/2 - 1), 1 kd (root n - 2)
+  unsigned long long *queue;  // [0] slot queue
+  int32_t *status;            // nonzero on overflow
+};
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+  return ax * bx + ay * by + az * bz;
+}
+
+// One row of a symmetric Q (xx, yy, zz, xy, xz, yz) dotted with r.
+__device__ __forceinline__ float qrow(const float *q, int i, float rx, float ry, float rz) {
+  if (i == 0) return q[0] * rx + q[3] * ry + q[4] * rz;
+  if (i == 1) return q[3] * rx + q[1] * ry + q[5] * rz;
+  return q[4] * rx + q[5] * ry + q[2] * rz;
+}
+
+// Far-field pair: monopole + Eq. 29 + Eq. 30 times 1/(4 pi |r|^3), and the
+// Eq. 14 estimate with the same factor (compute_link.cpp:608-627, :411-524).
+// Node 1 = u (moments m1 = "C" in the reference), node 2 = v ("D").
+__device__ void far_eval(const NodeMom &m1, const NodeMom &m2, float rx, float ry, float rz, double dsq, float r1,
+                         float r2, double &sum, double &err) {
+  const float *C3 = m1.D, *D3 = m2.D;
+  const float C1x = m1.t[0], C1y = m1.t[1], C1z = m1.t[2];
+  const float D1x = m2.t[0], D1y = m2.t[1], D1z = m2.t[2];
+  const float rdist2 = (float)(1.0 / dsq);
+  // monopole r . (c2 x c1)
+  float res = rx * (D1y * C1z - D1z * C1y) + ry * (D1z * C1x - D1x * C1z) + rz * (D1x * C1y - D1y * C1x);
+  // dipole (Eq. 29)
+  const float D2x = D3[5] - D3[7], D2y = D3[6] - D3[2], D2z = D3[1] - D3[3];
+  const float C2x = C3[5] - C3[7], C2y = C3[6] - C3[2], C2z = C3[1] - C3[3];
+  float ho = -(dot3(C1x, C1y, C1z, D2x, D2y, D2z) + dot3(C2x, C2y, C2z, D1x, D1y, D1z));
+  const float Dr0 = D3[0] * rx + D3[1] * ry + D3[2] * rz, Dr1 = D3[3] * rx + D3[4] * ry + D3[5] * rz,
+              Dr2 = D3[6] * rx + D3[7] * ry + D3[8] * rz;
+  const float Cr0 = C3[0] * rx + C3[1] * ry + C3[2] * rz, Cr1 = C3[3] * rx + C3[4] * ry + C3[5] * rz,
+              Cr2 = C3[6] * rx + C3[7] * ry + C3[8] * rz;
+  // (D3 r) x C1 . r  and  (C3 r) x D1 . r
+  const float t1 = rx * (Dr1 * C1z - Dr2 * C1y) + ry * (Dr2 * C1x - Dr0 * C1z) + rz * (Dr0 * C1y - Dr1 * C1x);
+  const float t2 = rx * (Cr1 * D1z - Cr2 * D1y) + ry * (Cr2 * D1x - Cr0 * D1z) + rz * (Cr0 * D1y - Cr1 * D1x);
+  ho -= 3.f * rdist2 * (t1 + t2);
+  // quadrupole (Eq. 30)
+  const float *P0 = m1.Q, *P1 = m1.Q + 6, *P2 = m1.Q + 12;
+  const float *Q0 = m2.Q, *Q1 = m2.Q + 6, *Q2 = m2.Q + 12;
+  const float ppx = P0[0] + P0[1] + P0[2], ppy = P1[0] + P1[1] + P1[2], ppz = P2[0] + P2[1] + P2[2];
+  const float qqx = Q0[0] + Q0[1] + Q0[2], qqy = Q1[0] + Q1[1] + Q1[2], qqz = Q2[0] + Q2[1] + Q2[2];
+  // -(r . (pp x D1 + C1 x qq))
+  const float sx = (ppy * D1z - ppz * D1y) + (C1y * qqz - C1z * qqy);
+  const float sy = (ppz * D1x - ppx * D1z) + (C1z * qqx - C1x * qqz);
+  const float sz = (ppx * D1y - ppy * D1x) + (C1x * qqy - C1y * qqx);
+  const float tqs1 = -(rx * sx + ry * sy + rz * sz);
+  const float p01 = dot3(C3[0], C3[1], C3[2], D3[3], D3[4], D3[5]);
+  const float p02 = dot3(C3[0], C3[1], C3[2], D3[6], D3[7], D3[8]);
+  const float p10 = dot3(C3[3], C3[4], C3[5], D3[0], D3[1], D3[2]);
+  const float p12 = dot3(C3[3], C3[4], C3[5], D3[6], D3[7], D3[8]);
+  const float p20 = dot3(C3[6], C3[7], C3[8], D3[0], D3[1], D3[2]);
+  const float p21 = dot3(C3[6], C3[7], C3[8], D3[3], D3[4], D3[5]);
+  const float tqs2 = 2.f * (rx * (p12 - p21) + ry * (p20 - p02) + rz * (p01 - p10));
+  const float tqs = tqs1 + tqs2;
+  const float pXx = qrow(P1, 2, rx, ry, rz) - qrow(P2, 1, rx, ry, rz);
+  const float pXy = qrow(P2, 0, rx, ry, rz) - qrow(P0, 2, rx, ry, rz);
+  const float pXz = qrow(P0, 1, rx, ry, rz) - qrow(P1, 0, rx, ry, rz);
+  float tqt = dot3(D1x, D1y, D1z, pXx, pXy, pXz);
+  const float qXx = qrow(Q1, 2, rx, ry, rz) - qrow(Q2, 1, rx, ry, rz);
+  const float qXy = qrow(Q2, 0, rx, ry, rz) - qrow(Q0, 2, rx, ry, rz);
+  const float qXz = qrow(Q0, 1, rx, ry, rz) - qrow(Q1, 0, rx, ry, rz);
+  tqt -= dot3(C1x, C1y, C1z, qXx, qXy, qXz);
+  // r . (C3^T D2 - D3^T C2)
+  const float ux = (C3[0] * D2x + C3[3] * D2y + C3[6] * D2z) - (D3[0] * C2x + D3[3] * C2y + D3[6] * C2z);
+  const float uy = (C3[1] * D2x + C3[4] * D2y + C3[7] * D2z) - (D3[1] * C2x + D3[4] * C2y + D3[7] * C2z);
+  const float uz = (C3[2] * D2x + C3[5] * D2y + C3[8] * D2z) - (D3[2] * C2x + D3[5] * C2y + D3[8] * C2z);
+  tqt += rx * ux + ry * uy + rz * uz;
+  // r^T Q r for each k
+  const float a0 = rx * qrow(P0, 0, rx, ry, rz) + ry * qrow(P0, 1, rx, ry, rz) + rz * qrow(P0, 2, rx, ry, rz);
+  const float a1 = rx * qrow(P1, 0, rx, ry, rz) + ry * qrow(P1, 1, rx, ry, rz) + rz * qrow(P1, 2, rx, ry, rz);
+  const float a2 = rx * qrow(P2, 0, rx, ry, rz) + ry * qrow(P2, 1, rx, ry, rz) + rz * qrow(P2, 2, rx, ry, rz);
+  const float b0 = rx * qrow(Q0, 0, rx, ry, rz) + ry * qrow(Q0, 1, rx, ry, rz) + rz * qrow(Q0, 2, rx, ry, rz);
+  const float b1 = rx * qrow(Q1, 0, rx, ry, rz) + ry * qrow(Q1, 1, rx, ry, rz) + rz * qrow(Q1, 2, rx, ry, rz);
+  const float b2 = rx * qrow(Q2, 0, rx, ry, rz) + ry * qrow(Q2, 1, rx, ry, rz) + rz * qrow(Q2, 2, rx, ry, rz);
+  // -r . (D1 x a) ; r . (C1 x b)
+  const float tfpp = -(rx * (D1y * a2 - D1z * a1) + ry * (D1z * a0 - D1x * a2) + rz * (D1x * a1 - D1y * a0));
+  const float tfqq = rx * (C1y * b2 - C1z * b1) + ry * (C1z * b0 - C1x * b2) + rz * (C1x * b1 - C1y * b0);
+  // 2 (C3 r) . (r x (D3 r))
+  const float wx = ry * Dr2 - rz * Dr1, wy = rz * Dr0 - rx * Dr2, wz = rx * Dr1 - ry * Dr0;
+  const float tfpq = 2.f * (Cr0 * wx + Cr1 * wy + Cr2 * wz);
+  const float tf = tfpp + tfqq + tfpq;
+  ho -= 1.5f * rdist2 * ((tqs + 2.f * tqt) + 5.f * rdist2 * tf);
+  const double mult = 1.0 / (dsq * sqrt(dsq)) * kInvFourPi;
+  sum += mult * ((double)res + (double)ho);
+  const float e = rdist2 * (m1.qn * (r1 * m2.tn + 3.f * m2.dn) + m2.qn * (r2 * m1.tn + 3.f * m1.dn));
+  err += mult * (double)e;
+}
+
+// Exact term of two segments in FP64 from their vertices (full turns).
+__device__ __noinline__ double seg_term_fp64(const double *xyz, int64_t p0i, int64_t p1i, int64_t q0i, int64_t q1i) {
+  double p0[3], p1[3], q0[3], q1[3];
+  for (int a = 0; a < 3; ++a) {
+    p0[a] = xyz[3 * p0i + a];
+    p1[a] = xyz[3 * p1i + a];
+    q0[a] = xyz[3 * q0i + a];
+    q1[a] = xyz[3 * q1i + a];
+  }
+  // Midpoint/tangent form of compute_link.cpp:578-605.
+  const double m1[3] = {0.5 * p0[0] + 0.5 * p1[0], 0.5 * p0[1] + 0.5 * p1[1], 0.5 * p0[2] + 0.5 * p1[2]};
+  const double m2[3] = {0.5 * q0[0] + 0.5 * q1[0], 0.5 * q0[1] + 0.5 * q1[1], 0.5 * q0[2] + 0.5 * q1[2]};
+  const double t1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+  const double t2[3] = {q1[0] - q0[0], q1[1] - q0[1], q1[2] - q0[2]};
+  const double dr[3] = {m2[0] - m1[0], m2[1] - m1[1], m2[2] - m1[2]};
+  const double det = dr[0] * (t2[1] * t1[2] - t2[2] * t1[1]) + dr[1] * (t2[2] * t1[0] - t2[0] * t1[2]) +
+                     dr[2] * (t2[0] * t1[1] - t2[1] * t1[0]);
+  double al[3], be[3], ga[3], de[3];
+  for (int a = 0; a < 3; ++a) {
+    al[a] = dr[a] + 0.5 * (t1[a] - t2[a]);
+    be[a] = dr[a] + 0.5 * (-t2[a] - t1[a]);
+    ga[a] = dr[a] + 0.5 * (t2[a] - t1[a]);
+    de[a] = dr[a] + 0.5 * (t2[a] + t1[a]);
+  }
+  auto dt = [](const double *x, const double *y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+  const double la = sqrt(dt(al, al)), lb = sqrt(dt(be, be)), lc = sqrt(dt(ga, ga)), ld = sqrt(dt(de, de));
+  const double ac = dt(al, ga);
+  const double div1 = la * lb * lc + dt(al, be) * lc + ac * lb + dt(be, ga) * la;
+  const double div2 = la * ld * lc + dt(al, de) * lc + ac * ld + dt(de, ga) * la;
+  const double x = div1 * div2 - det * det;
+  const double s = (det == 0) ? copysign(1.0, div1) + copysign(1.0, div2) : (div1 + div2);
+  const double y = det * s;
+  const double sg = (det == 0) ? -copysign(1.0, div1) : copysign(1.0, det);
+  return kInvTwoPi * atan2(y, x) + (((s < 0) || ((s == 0) && (det < 0))) ? sg : 0.0);
+}
+
+// Exact leaf-leaf term in FP32 from the separation and the two tangents
+// (compute_link.cpp:576-606); FP64 from the vertices when the segments are
+// closer than their length.
+__device__ void leaf_eval(const TravArgs &A, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &m1,
+                          const NodeMom &m2, int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
+  const float rx = (float)(h2.m[0] - h1.m[0]), ry = (float)(h2.m[1] - h1.m[1]), rz = (float)(h2.m[2] - h1.m[2]);
+  const float t1x = m1.t[0], t1y = m1.t[1], t1z = m1.t[2];
+  const float t2x = m2.t[0], t2y = m2.t[1], t2z = m2.t[2];
+  const float alx = rx + 0.5f * (t1x - t2x), aly = ry + 0.5f * (t1y - t2y), alz = rz + 0.5f * (t1z - t2z);
+  const float bex = rx - 0.5f * (t2x + t1x), bey = ry - 0.5f * (t2y + t1y), bez = rz - 0.5f * (t2z + t1z);
+  const float gax = rx + 0.5f * (t2x - t1x), gay = ry + 0.5f * (t2y - t1y), gaz = rz + 0.5f * (t2z - t1z);
+  const float dex = rx + 0.5f * (t2x + t1x), dey = ry + 0.5f * (t2y + t1y), dez = rz + 0.5f * (t2z + t1z);
+  const float la = sqrtf(dot3(alx, aly, alz, alx, aly, alz)), lb = sqrtf(dot3(bex, bey, bez, bex, bey, bez));
+  const float lc = sqrtf(dot3(gax, gay, gaz, gax, gay, gaz)), ld = sqrtf(dot3(dex, dey, dez, dex, dey, dez));
+  if (fminf(fminf(la, lb), fminf(lc, ld)) < fmaxf(m1.tn, m2.tn)) {
+    const int64_t s1 = -1 - h1.left, s2 = -1 - h2.left;
+    sum += seg_term_fp64(A.xyz, o1 + s1, o1 + (s1 + 1 == n1 ? 0 : s1 + 1), o2 + s2, o2 + (s2 + 1 == n2 ? 0 : s2 + 1));
+    return;
+  }
+  const float det = rx * (t2y * t1z - t2z * t1y) + ry * (t2z * t1x - t2x * t1z) + rz * (t2x * t1y - t2y * t1x);
+  const float ac = dot3(alx, aly, alz, gax, gay, gaz);
+  const float div1 = la * lb * lc + dot3(alx, aly, alz, bex, bey, bez) * lc + ac * lb + dot3(bex, bey, bez, gax, gay, gaz) * la;
+  const float div2 = la * ld * lc + dot3(alx, aly, alz, dex, dey, dez) * lc + ac * ld + dot3(dex, dey, dez, gax, gay, gaz) * la;
+  const float x = div1 * div2 - det * det;
+  const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
+  const float y = det * s;
+  const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
+  sum += kInvTwoPi * (double)atan2f(y, x) + (((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? (double)sg : 0.0);
+}
+
+__global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
+  __shared__ int2 s_stack[kWarps][kStack];
+  __shared__ int2 s_far[kWarps][64];
+  __shared__ int2 s_leaf[kWarps][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + w;
+  int2 *stack = s_stack[w];
+  int2 *farq = s_far[w];
+  int2 *leafq = s_leaf[w];
+  int2 *spill = A.spill + (size_t)gw * kSpill;
+  double nfar = 0, nleaf = 0;
+  for (;;) {
+    int slot = 0;
+    if (lane == 0) slot = (int)atomicAdd(A.queue, 1ULL);
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if (slot >= A.nslots) break;
+    const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+    const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
+    const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
+    const NodeMom *M1 = A.mom + A.node_base[l1], *M2 = A.mom + A.node_base[l2];
+    const double itolsq = A.itolsq[slot], eps = A.epssq;
+    int top = 0, nspill = 0, nf = 0, nl = 0;
+    bool overflow = false;
+    if (lane == 0)
+      stack[0] = A.tree_kind == 0 ? make_int2((int)(n1 / 2 - 1), (int)(n2 / 2 - 1))
+                                  : make_int2((int)(n1 - 2), (int)(n2 - 2));  // roots
+    top = 1;
+    double sum = 0.0, err = 0.0;
+    __syncwarp();
+    while (true) {
+      if (top == 0 && nspill > 0) {  // refill from the spill buffer
+        const int k = min(nspill, kStack / 2);
+        for (int x = lane; x < k; x += 32) stack[x] = spill[nspill - k + x];
+        nspill -= k;
+        top = k;
+        __syncwarp();
+      }
+      if (top == 0) break;
+      const int cnt = min(top, 32);
+      const bool act = lane < cnt;
+      int2 pr = make_int2(0, 0);
+      if (act) pr = stack[top - cnt + lane];
+      __syncwarp();
+      top -= cnt;
+      int kind = 0;  // 0 none, 1 leaf, 2 far, 3 split
+      int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
+      if (act) {
+        const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+        const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
+        const double rs = h1.r + h2.r;
+        if (leaf1 && leaf2) {
+          kind = 1;
+        } else if (dx * dx + dy * dy + dz * dz + eps > rs * rs * itolsq + eps) {
+          kind = 2;
+        } else {
+          kind = 3;
+          const bool split2 = (!leaf1 && !leaf2) ? (h2.rsq > h1.rsq) : !leaf2;
+          if (split2) {
+            c0 = make_int2(pr.x, h2.left);
+            c1 = make_int2(pr.x, h2.right);
+          } else {
+            c0 = make_int2(h1.left, pr.y);
+            c1 = make_int2(h1.right, pr.y);
+          }
+        }
+      }
+      // push children
+      const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
+      const int ns = __popc(sm);
+      if (top + 2 * ns > kStack) {  // spill the oldest half
+        const int k = top / 2;
+        if (nspill + k > kSpill) {
+          overflow = true;
+          break;
+        }
+        for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
+        __syncwarp();
+        // k >= kStack / 2 - 32 > 32, so no pass reads what an earlier write covered.
+        for (int x = lane; x < top - k; x += 32) stack[x] = stack[k + x];
+        nspill += k;
+        top -= k;
+        __syncwarp();
+      }
+      if (kind == 3) {
+        const int rank = __popc(sm & ((1u << lane) - 1));
+        stack[top + 2 * rank] = c0;
+        stack[top + 2 * rank + 1] = c1;
+      }
+      top += 2 * ns;
+      // queue far and leaf pairs
+      const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
+      const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
+      if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
+      if (kind == 1) leafq[nl + __popc(lm & ((1u << lane) - 1))] = pr;
+      nf += __popc(fm);
+      nl += __popc(lm);
+      __syncwarp();
+      const bool drain = (top == 0 && nspill == 0);
+      while (nf >= 32 || (drain && nf > 0)) {
+        const int k = min(nf, 32);
+        if (lane < k) {
+          const int2 q = farq[nf - k + lane];
+          const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+          const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+          const double dsq = dx * dx + dy * dy + dz * dz + eps;
+          far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dsq, (float)h1.r, (float)h2.r, sum, err);
+        }
+        nfar += k;
+        nf -= k;
+        __syncwarp();
+      }
+      while (nl >= 32 || (drain && nl > 0)) {
+        const int k = min(nl, 32);
+        if (lane < k) {
+          const int2 q = leafq[nl - k + lane];
+          leaf_eval(A, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+        }
+        nleaf += k;
+        nl -= k;
+        __syncwarp();
+      }
+    }
+    if (overflow && lane == 0) atomicExch(A.status, 1);
+    for (int o = 16; o; o >>= 1) {
+      sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      err += __shfl_xor_sync(0xffffffffu, err, o);
+    }
+    if (lane == 0) {
+      const int p = A.slot_pair[slot];
+      A.lk[p] = overflow ? __longlong_as_double(0x7ff8000000000000LL) : sum;
+      A.err[p] = err;
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(A.counts, nfar);
+    atomicAdd(A.counts + 1, nleaf);
+  }
+}
+
+__global__ void scatter_kernel(const double *src, const int32_t *idx, int64_t n, double *dst) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) dst[idx[k]] = src[k];
+}
+
+// Host kd-median tree (ModifiedKdBVH.h:101-132, :207-237), for bh_tree = 1:
+// children in local ids, leaf_seg per leaf position.
+void host_kd_tree(const double *xyz, int64_t n, std::vector<int32_t> &children, std::vector<int32_t> &leaf_seg) {
+  std::vector<double> lo(3 * n), hi(3 * n), cen(3 * n);
+  for (int64_t s = 0; s < n; ++s) {
+    const double *p = xyz + 3 * s, *q = xyz + 3 * ((s + 1) % n);
+    for (int a = 0; a < 3; ++a) {
+      lo[3 * s + a] = std::min(p[a], q[a]);
+      hi[3 * s + a] = std::max(p[a], q[a]);
+      cen[3 * s + a] = (lo[3 * s + a] + hi[3 * s + a]) / 2.0;
+    }
+  }
+  std::vector<int32_t> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  children.assign(2 * (n - 1), 0);
+  int32_t next = 0;
+  struct R {
+    std::vector<int32_t> &idx, &ch;
+    const std::vector<double> &cen;
+    int32_t &next;
+    int64_t n;
+    int32_t go(int64_t from, int64_t to, int dim) {
+      auto cmp = [&](int32_t a, int32_t b) { return cen[3 * a + dim] < cen[3 * b + dim]; };
+      const int64_t size = to - from;
+      int32_t l, r;
+      if (size == 2) {
+        l = (int32_t)(from + n - 1);
+        r = (int32_t)(from + n);
+      } else if (size == 3) {
+        const int64_t mid = from + 2;
+        std::nth_element(idx.begin() + from, idx.begin() + mid, idx.begin() + to, cmp);
+        l = go(from, mid, (dim + 1) % 3);
+        r = (int32_t)(mid + n - 1);
+      } else {
+        const int64_t mid = from + size / 2;
+        std::nth_element(idx.begin() + from, idx.begin() + mid, idx.begin() + to, cmp);
+        l = go(from, mid, (dim + 1) % 3);
+        r = go(mid, to, (dim + 1) % 3);
+      }
+      const int32_t me = next++;
+      ch[2 * me] = l;
+      ch[2 * me + 1] = r;
+      return me;
+    }
+  } rec{idx, children, cen, next, n};
+  rec.go(0, n, 0);
+  leaf_seg = idx;
+}
+
+__global__ void parents_from_children(const int32_t *children, const int64_t *node_base, const int64_t *off,
+                                      const int32_t *loops, int32_t nloops, const int64_t *seg_start,
+                                      int64_t total_internal, int32_t *parent, int32_t *arrive) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total_internal) return;
+  const int k = find_loop_of(seg_start, nloops, g);
+  const int l = loops[k];
+  const int64_t base = node_base[l];
+  const int32_t node = (int32_t)(g - seg_start[k]);
+  const int64_t n = off[l + 1] - off[l];
+  parent[base + children[2 * (base + node)]] = node;
+  parent[base + children[2 * (base + node) + 1]] = node;
+  arrive[base + node] = 0;
+  if (node == n - 2) parent[base + node] = -1;
+}
+
+}  // namespace
+
+void scatter_doubles(Context &ctx, const double *src, const int32_t *idx, int64_t n, double *dst) {
+  if (n <= 0) return;
+  scatter_kernel<<<(int)((n + 255) / 256), 256, 0, ctx.stream>>>(src, idx, n, dst);
+  FLN_CUDA(cudaGetLastError());
+}
+
+int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
+                      const std::vector<int32_t> &h_pairs, const fln_params &prm, double *d_lk_out,
+                      double *d_err_out, int32_t *d_flags_out) {
+  const int64_t np = (int64_t)h_pairs.size() / 2;
+  if (np == 0) return 0;
+  const int nl_all = (int)h_off.size() - 1;
+  // Loops that need a tree, their node bases and build index ranges.
+  std::vector<char> need(nl_all, 0);
+  for (int32_t l : h_pairs) need[l] = 1;
+  std::vector<int32_t> loops;
+  std::vector<int64_t> node_base(nl_all, 0), seg_int(1, 0), seg_all(1, 0);
+  int64_t nodes = 0;
+  int maxdepth = 0;
+  for (int l = 0; l < nl_all; ++l) {
+    if (!need[l]) continue;
+    const int64_t n = h_off[l + 1] - h_off[l];
+    loops.push_back(l);
+    node_base[l] = nodes;
+    nodes += 2 * n - 1;
+    seg_int.push_back(seg_int.back() + (n - 1));
+    seg_all.push_back(seg_all.back() + n);
+    int d = 0;
+    while ((int64_t(1) << d) < n) ++d;
+    maxdepth = std::max(maxdepth, d);
+  }
+  const int32_t nloops = (int32_t)loops.size();
+  const int64_t tot_int = seg_int.back(), tot_leaf = seg_all.back();
+  // Device buffers (grow-only).
+  int32_t *d_loops = ctx.d_bh[0].as<int32_t>(nloops);
+  int64_t *d_base = ctx.d_bh[1].as<int64_t>(nl_all);
+  int64_t *d_segint = ctx.d_bh[2].as<int64_t>(nloops + 1);
+  int64_t *d_segall = ctx.d_bh[3].as<int64_t>(nloops + 1);
+  int32_t *d_children = ctx.d_bh[4].as<int32_t>(2 * nodes);
+  int32_t *d_parent = ctx.d_bh[5].as<int32_t>(nodes);
+  int32_t *d_leafseg = ctx.d_bh[6].as<int32_t>(nodes);
+  int32_t *d_arrive = ctx.d_bh[7].as<int32_t>(nodes);
+  BuildNode *d_bn = ctx.d_bh[8].as<BuildNode>(nodes);
+  NodeHdr *d_hdr = ctx.d_bh[9].as<NodeHdr>(nodes);
+  NodeMom *d_mom = ctx.d_bh[10].as<NodeMom>(nodes);
+  cudaStream_t st = ctx.stream;
+  FLN_CUDA(cudaMemcpyAsync(d_loops, loops.data(), nloops * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  FLN_CUDA(cudaMemcpyAsync(d_base, node_base.data(), nl_all * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  FLN_CUDA(cudaMemcpyAsync(d_segint, seg_int.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  FLN_CUDA(cudaMemcpyAsync(d_segall, seg_all.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  TreeArgs T{d_xyz, d_off, d_base, d_loops, nloops, d_children, d_parent, d_leafseg, d_arrive, d_bn, d_hdr, d_mom};
+  int launches = 0;
+  FLN_CUDA(cudaEventRecord(ctx.ev2, st));
+  if (prm.bh_tree == 1) {
+    // The reference's kd-median tree, built on the host from a copy of the loops.
+    std::vector<int32_t> ch_all(2 * nodes, 0), ls_all(nodes, 0);
+    std::vector<double> xyz_host(3 * h_off.back());
+    FLN_CUDA(cudaMemcpyAsync(xyz_host.data(), d_xyz, xyz_host.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < nloops; ++k) {
+      const int l = loops[k];
+      const int64_t n = h_off[l + 1] - h_off[l];
+      std::vector<int32_t> ch, ls;
+      host_kd_tree(xyz_host.data() + 3 * h_off[l], n, ch, ls);
+      std::copy(ch.begin(), ch.end(), ch_all.begin() + 2 * node_base[l]);
+      for (int64_t p = 0; p < n; ++p) ls_all[node_base[l] + n - 1 + p] = ls[p];
+    }
+    FLN_CUDA(cudaMemcpyAsync(d_children, ch_all.data(), ch_all.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemcpyAsync(d_leafseg, ls_all.data(), ls_all.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    parents_from_children<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(d_children, d_base, d_off, d_loops, nloops,
+                                                                        d_segint, tot_int, d_parent, d_arrive);
+    FLN_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
+    ++launches;
+  } else {
+    curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int);
+    identity_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
+    launches += 2;
+  }
+  FLN_CUDA(cudaGetLastError());
+  build_moments<<<(int)((tot_leaf + 127) / 128), 128, 0, st>>>(T, d_segall, tot_leaf);
+  FLN_CUDA(cudaGetLastError());
+  FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+  ++launches;
+
+  // Traversal slots: order pairs by decreasing work.
+  std::vector<int32_t> order(np);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<double> cost(np);
+  for (int64_t p = 0; p < np; ++p) {
+    const double a = (double)(h_off[h_pairs[2 * p] + 1] - h_off[h_pairs[2 * p]]);
+    const double b = (double)(h_off[h_pairs[2 * p + 1] + 1] - h_off[h_pairs[2 * p + 1]]);
+    cost[p] = (a + b) * std::log2(a + b + 2.0);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  std::vector<int32_t> slot_loops(2 * np);
+  for (int64_t s = 0; s < np; ++s) {
+    slot_loops[2 * s] = h_pairs[2 * order[s]];
+    slot_loops[2 * s + 1] = h_pairs[2 * order[s] + 1];
+  }
+  int32_t *d_slots = ctx.d_bh[11].as<int32_t>(3 * np);
+  int32_t *d_slot_pair = d_slots + 2 * np;
+  double *d_itol = ctx.d_bh[12].as<double>(np);
+  double *d_counts = ctx.d_bh[13].as<double>(2);
+  int32_t *d_status = reinterpret_cast<int32_t *>(d_counts + 2);
+  unsigned long long *d_queue = ctx.d_counter.as<unsigned long long>(2);
+  int per_sm = 0;
+  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_traverse, 32 * kWarps, 0));
+  per_sm = std::max(per_sm, 1);
+  const int64_t want = std::max<int64_t>(1, std::min<int64_t>((np + kWarps - 1) / kWarps, (int64_t)ctx.num_sms * per_sm));
+  const int grid = (int)want;
+  int2 *d_spill = ctx.d_bh[14].as<int2>((size_t)grid * kWarps * kSpill);
+  FLN_CUDA(cudaMemcpyAsync(d_slots, slot_loops.data(), 2 * np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  FLN_CUDA(cudaMemcpyAsync(d_slot_pair, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  const double b0 = prm.barnes_hut_init_beta;
+  std::vector<double> itol(np, b0 * b0);
+  FLN_CUDA(cudaMemcpyAsync(d_itol, itol.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
+  FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
+  FLN_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), st));
+  ctx.stats.ms_tree_build = ctx.elapsed(ctx.ev2, ctx.ev3);
+  TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_slot_pair, d_itol, (int32_t)np, prm.epssq, d_lk_out,
+             d_err_out, d_counts, d_spill, prm.bh_tree == 1 ? 1 : 0, d_queue, d_status};
+  FLN_CUDA(cudaEventRecord(ctx.ev2, st));
+  bh_traverse<<<grid, 32 * kWarps, 0, st>>>(A);
+  FLN_CUDA(cudaGetLastError());
+  FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+  ++launches;
+  // Error estimate and beta retry (lnc.cpp:165-184).
+  std::vector<double> err(np);
+  FLN_CUDA(cudaMemcpyAsync(err.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  int32_t status = 0;
+  FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaStreamSynchronize(st));
+  ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+  std::vector<int32_t> flags(np, 0), rs_loops, rs_pair;
+  std::vector<double> rs_itol;
+  for (int64_t p = 0; p < np; ++p) {
+    const double e = err[p] * prm.error_est_scale;
+    err[p] = e;
+    const double tb = std::min(std::pow(e / prm.target_error, 0.25) * b0, prm.barnes_hut_beta_limit);
+    if (tb > b0) {
+      rs_loops.push_back(h_pairs[2 * p]);
+      rs_loops.push_back(h_pairs[2 * p + 1]);
+      rs_pair.push_back((int32_t)p);
+      rs_itol.push_back(tb * tb);
+      flags[p] |= FLN_PAIR_BETA_RETRIED;
+    }
+  }
+  std::vector<double> far_leaf(2, 0.0);
+  if (!rs_pair.empty()) {
+    const int64_t nr = (int64_t)rs_pair.size();
+    FLN_CUDA(cudaMemcpyAsync(d_slots, rs_loops.data(), 2 * nr * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemcpyAsync(d_slot_pair, rs_pair.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemcpyAsync(d_itol, rs_itol.data(), nr * sizeof(double), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), st));
+    TravArgs R = A;
+    R.nslots = (int32_t)nr;
+    const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>((nr + kWarps - 1) / kWarps, grid));
+    FLN_CUDA(cudaEventRecord(ctx.ev2, st));
+    bh_traverse<<<g2, 32 * kWarps, 0, st>>>(R);
+    FLN_CUDA(cudaGetLastError());
+    FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+    ++launches;
+    // After a retry the reference keeps the new run's unscaled estimate.
+    std::vector<double> e2(np);
+    FLN_CUDA(cudaMemcpyAsync(e2.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+    for (int32_t p : rs_pair) err[p] = e2[p];
+    ctx.stats.beta_retried = nr;
+    ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+  } else {
+    ctx.stats.beta_retried = 0;
+  }
+  FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(d_err_out, err.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (d_flags_out) FLN_CUDA(cudaMemcpyAsync(d_flags_out, flags.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  FLN_CUDA(cudaStreamSynchronize(st));
+  ctx.stats.bh_far_evals = far_leaf[0];
+  ctx.stats.bh_leaf_evals = far_leaf[1];
+  if (status != 0)
+    throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
+                                            std::to_string(maxdepth) + ").");
+  return launches;
+}
+
+}  // namespace fln

@@ -1,0 +1,564 @@
+// The C ABI of include/fln.h: argument checks, host<->device staging, the
+// FP64 recompute of low-margin pairs, certificates. No exception crosses it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace fln {
+
+Context::Context(int dev, void *user_stream) : device(dev) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw Error(FLN_ERR_NO_DEVICE, "No CUDA device is visible.");
+  if (dev < 0 || dev >= n) throw Error(FLN_ERR_INVALID_ARGUMENT, "Device index out of range.");
+  FLN_CUDA(cudaSetDevice(dev));
+  FLN_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  if (user_stream) {
+    stream = static_cast<cudaStream_t>(user_stream);
+  } else {
+    FLN_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  FLN_CUDA(cudaEventCreate(&ev0));
+  FLN_CUDA(cudaEventCreate(&ev1));
+  FLN_CUDA(cudaEventCreate(&ev2));
+  FLN_CUDA(cudaEventCreate(&ev3));
+}
+
+Context::~Context() {
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (DevBuf *b : {&d_xyz, &d_off, &d_pairs, &d_loops, &d_items, &d_partial, &d_counter, &d_lk, &d_err, &d_flags,
+                    &d_near})
+    b->release();
+  for (auto &b : d_bh) b.release();
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (ev2) cudaEventDestroy(ev2);
+  if (ev3) cudaEventDestroy(ev3);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+// Scatters src[k] into dst[idx[k]] for the FP64 recompute (defined in bh.cu).
+void scatter_doubles(Context &ctx, const double *src, const int32_t *idx, int64_t n, double *dst);
+
+// Runs the requested method over device-resident loops and pairs, then the
+// margin check and FP64 direct-sum recompute of the pairs that fail it.
+static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
+                     const std::vector<int32_t> &h_pairs, fln_method method, const fln_params &prm,
+                     double *d_lk, double *d_err, int32_t *d_flags) {
+  const int64_t np = (int64_t)h_pairs.size() / 2;
+  int launches = 0;
+  double near_terms = 0;
+  ctx.stats.ms_main_kernel = 0;
+  ctx.stats.ms_tree_build = 0;
+  ctx.stats.bh_far_evals = ctx.stats.bh_leaf_evals = 0;
+  ctx.stats.beta_retried = 0;
+  if (!d_err) d_err = ctx.d_err.as<double>(std::max<int64_t>(np, 1));  // Barnes–Hut needs one
+  if (method == FLN_METHOD_DIRECTSUM) {
+    launches += direct_sum_device(ctx, d_xyz, d_off, h_off, h_pairs, prm.precision, prm.near_factor, d_lk,
+                                  prm.precision == FLN_PREC_MIXED ? &near_terms : nullptr);
+    if (d_err) FLN_CUDA(cudaMemsetAsync(d_err, 0, np * sizeof(double), ctx.stream));
+    if (d_flags) FLN_CUDA(cudaMemsetAsync(d_flags, 0, np * sizeof(int32_t), ctx.stream));
+  } else {
+    launches += barnes_hut_device(ctx, d_xyz, d_off, h_off, h_pairs, prm, d_lk, d_err, d_flags);
+  }
+  ctx.stats.near_fp64_terms = near_terms;
+  const bool checked = !(method == FLN_METHOD_DIRECTSUM && prm.precision == FLN_PREC_FP64);
+  ctx.stats.fp64_recomputed = 0;
+  if (checked && np > 0) {
+    std::vector<double> lk(np), err(np, 0.0);
+    FLN_CUDA(cudaMemcpyAsync(lk.data(), d_lk, np * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    if (d_err) FLN_CUDA(cudaMemcpyAsync(err.data(), d_err, np * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+    std::vector<int32_t> redo_idx, redo_pairs;
+    for (int64_t p = 0; p < np; ++p) {
+      const double r = std::round(lk[p]);
+      const double margin = 0.5 - std::fabs(lk[p] - r);
+      // Low margin, non-finite, or a Barnes–Hut error estimate that could
+      // reach the rounding boundary: recompute in FP64 direct sum.
+      if (!(margin >= prm.fp64_margin) || !(err[p] <= 0.5 - prm.fp64_margin)) {
+        redo_idx.push_back((int32_t)p);
+        redo_pairs.push_back(h_pairs[2 * p]);
+        redo_pairs.push_back(h_pairs[2 * p + 1]);
+      }
+    }
+    if (!redo_idx.empty()) {
+      const int64_t nr = (int64_t)redo_idx.size();
+      double *d_tmp = ctx.d_near.as<double>(nr + nr / 2 + 2);
+      int32_t *d_idx = reinterpret_cast<int32_t *>(d_tmp + nr);
+      launches += direct_sum_device(ctx, d_xyz, d_off, h_off, redo_pairs, FLN_PREC_FP64, 0.0, d_tmp, nullptr);
+      FLN_CUDA(cudaMemcpyAsync(d_idx, redo_idx.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, ctx.stream));
+      scatter_doubles(ctx, d_tmp, d_idx, nr, d_lk);
+      ++launches;
+      if (d_flags) {
+        std::vector<int32_t> fl(np, 0);
+        FLN_CUDA(cudaMemcpyAsync(fl.data(), d_flags, np * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+        FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+        for (int32_t p : redo_idx) fl[p] |= FLN_PAIR_FP64_RECOMPUTED;
+        FLN_CUDA(cudaMemcpyAsync(d_flags, fl.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, ctx.stream));
+      }
+      ctx.stats.fp64_recomputed = nr;
+    }
+  }
+  double sp = 0;
+  for (int64_t p = 0; p < np; ++p)
+    sp += (double)(h_off[h_pairs[2 * p] + 1] - h_off[h_pairs[2 * p]]) *
+          (double)(h_off[h_pairs[2 * p + 1] + 1] - h_off[h_pairs[2 * p + 1]]);
+  ctx.stats.segment_pairs = sp;
+  ctx.stats.pairs = np;
+  return launches;
+}
+
+static void check_inputs(const std::vector<int64_t> &h_off, int32_t nloops, const std::vector<int32_t> &h_pairs) {
+  if (h_off.size() != (size_t)nloops + 1 || h_off[0] != 0)
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "loop_offsets must start at 0 and hold nloops + 1 entries.");
+  for (int32_t l = 0; l < nloops; ++l)
+    if (h_off[l + 1] < h_off[l]) throw Error(FLN_ERR_INVALID_ARGUMENT, "loop_offsets must be non-decreasing.");
+  for (size_t k = 0; k < h_pairs.size(); ++k) {
+    const int32_t l = h_pairs[k];
+    if (l < 0 || l >= nloops) throw Error(FLN_ERR_INVALID_ARGUMENT, "pair index out of range.");
+    if (h_off[l + 1] - h_off[l] < 2)
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "every loop in a pair needs at least two vertices.");
+  }
+  for (size_t p = 0; p + 1 < h_pairs.size(); p += 2)
+    if (h_pairs[p] == h_pairs[p + 1]) throw Error(FLN_ERR_INVALID_ARGUMENT, "a pair must name two different loops.");
+}
+
+static fln_params resolved(const fln_params *p) {
+  fln_params r;
+  fln_default_params(&r);
+  if (p) r = *p;
+  if (r.precision != FLN_PREC_FP64 && r.precision != FLN_PREC_MIXED)
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (!(r.barnes_hut_init_beta > 0) || !(r.barnes_hut_beta_limit > 0))
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "Barnes-Hut beta must be positive");
+  return r;
+}
+
+}  // namespace fln
+
+using namespace fln;
+
+struct fln_ctx {
+  std::unique_ptr<Context> c;
+};
+struct fln_model {
+  Model m;
+  int prepared_disc = -1;
+};
+struct fln_certificate {
+  Certificate c;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <class F>
+fln_status guarded(F &&f) {
+  try {
+    f();
+    return FLN_OK;
+  } catch (const Error &e) {
+    g_last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host out of memory";
+    return FLN_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return FLN_ERR_INTERNAL;
+  }
+}
+
+void compute_pairs_host(Context &ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                        const int32_t *pairs, int64_t npairs, fln_method method, const fln_params &prm,
+                        double *lk_out, double *err_out, int32_t *flags_out) {
+  const double t0 = now_ms();
+  FLN_CUDA(cudaSetDevice(ctx.device));
+  std::vector<int64_t> h_off(loop_offsets, loop_offsets + nloops + 1);
+  std::vector<int32_t> h_pairs(pairs, pairs + 2 * npairs);
+  check_inputs(h_off, nloops, h_pairs);
+  const int64_t nv = h_off[nloops];
+  double *d_xyz = ctx.d_xyz.as<double>(3 * std::max<int64_t>(nv, 1));
+  int64_t *d_off = ctx.d_off.as<int64_t>(nloops + 1);
+  double *d_lk = ctx.d_lk.as<double>(std::max<int64_t>(npairs, 1));
+  double *d_err = ctx.d_err.as<double>(std::max<int64_t>(npairs, 1));
+  int32_t *d_flags = ctx.d_flags.as<int32_t>(std::max<int64_t>(npairs, 1));
+  FLN_CUDA(cudaEventRecord(ctx.ev0, ctx.stream));
+  FLN_CUDA(cudaMemcpyAsync(d_xyz, xyz, 3 * nv * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+  FLN_CUDA(cudaMemcpyAsync(d_off, h_off.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+  const int launches = run_pairs(ctx, d_xyz, d_off, h_off, h_pairs, method, prm, d_lk, d_err, d_flags);
+  FLN_CUDA(cudaEventRecord(ctx.ev1, ctx.stream));
+  FLN_CUDA(cudaMemcpyAsync(lk_out, d_lk, npairs * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+  if (err_out) FLN_CUDA(cudaMemcpyAsync(err_out, d_err, npairs * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+  if (flags_out)
+    FLN_CUDA(cudaMemcpyAsync(flags_out, d_flags, npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+  FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1);
+  ctx.stats.ms_kernels = ms;
+  ctx.stats.kernel_launches = launches;
+  ctx.stats.ms_total = now_ms() - t0;
+}
+}  // namespace
+
+extern "C" {
+
+const char *fln_status_string(fln_status s) {
+  switch (s) {
+    case FLN_OK: return "ok";
+    case FLN_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case FLN_ERR_IO: return "i/o error";
+    case FLN_ERR_FORMAT: return "format error";
+    case FLN_ERR_CUDA: return "CUDA error";
+    case FLN_ERR_NO_DEVICE: return "no CUDA device";
+    case FLN_ERR_OUT_OF_MEMORY: return "out of memory";
+    case FLN_ERR_SEGMENT_TOO_SMALL: return "segment smaller than eps * average coordinate";
+    case FLN_ERR_MAX_RECURSION: return "Discretize reached its maximum number of rounds";
+    case FLN_ERR_UNLOOPED: return "open curve in the linking-number stage";
+    case FLN_ERR_NONFINITE: return "non-finite linking number";
+    case FLN_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+    case FLN_ERR_TIMEOUT: return "bounded device wait ran out";
+    default: return "internal error";
+  }
+}
+
+const char *fln_last_error(void) { return g_last_error.c_str(); }
+int fln_abi_version(void) { return FLN_ABI_VERSION; }
+
+void fln_default_params(fln_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->barnes_hut_init_beta = 2.0;
+  p->barnes_hut_beta_limit = 10.0;
+  p->epssq = 1e-24;
+  p->target_error = 0.1;
+  p->error_est_scale = 0.05;
+  p->precision = FLN_PREC_MIXED;
+  p->fp64_margin = 0.25;
+  p->near_factor = 1.0;
+  p->bh_tree = 0;
+}
+
+fln_status fln_ctx_create(int device, void *stream, fln_ctx **out) {
+  return guarded([&] {
+    if (!out) throw Error(FLN_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    auto *c = new fln_ctx;
+    try {
+      c->c.reset(new Context(device, stream));
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+void fln_ctx_destroy(fln_ctx *ctx) { delete ctx; }
+
+fln_status fln_ctx_stats(const fln_ctx *ctx, fln_stats *out) {
+  return guarded([&] {
+    if (!ctx || !out) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = ctx->c->stats;
+  });
+}
+
+fln_status fln_linking_numbers(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                               const int32_t *pairs, int64_t npairs, fln_method method, const fln_params *params,
+                               double *lk_out, double *err_out, int32_t *flags_out) {
+  return guarded([&] {
+    if (!ctx || !loop_offsets || nloops < 0 || npairs < 0 || (npairs && (!pairs || !lk_out)) ||
+        (!xyz && nloops && loop_offsets[nloops] > 0))
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL or negative argument");
+    if (method != FLN_METHOD_DIRECTSUM && method != FLN_METHOD_BARNESHUT)
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "Invalid method");
+    const fln_params prm = resolved(params);
+    compute_pairs_host(*ctx->c, xyz, loop_offsets, nloops, pairs, npairs, method, prm, lk_out, err_out, flags_out);
+  });
+}
+
+fln_status fln_linking_numbers_device(fln_ctx *ctx, const double *d_xyz, const int64_t *d_loop_offsets,
+                                      int32_t nloops, const int32_t *d_pairs, int64_t npairs, fln_method method,
+                                      const fln_params *params, double *d_lk_out, double *d_err_out,
+                                      int32_t *d_flags_out) {
+  return guarded([&] {
+    if (!ctx || !d_loop_offsets || nloops < 0 || npairs < 0 || (npairs && (!d_pairs || !d_lk_out)))
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL or negative argument");
+    if (method != FLN_METHOD_DIRECTSUM && method != FLN_METHOD_BARNESHUT)
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "Invalid method");
+    const fln_params prm = resolved(params);
+    Context &c = *ctx->c;
+    const double t0 = now_ms();
+    FLN_CUDA(cudaSetDevice(c.device));
+    std::vector<int64_t> h_off(nloops + 1);
+    std::vector<int32_t> h_pairs(2 * npairs);
+    FLN_CUDA(cudaEventRecord(c.ev0, c.stream));
+    FLN_CUDA(cudaMemcpyAsync(h_off.data(), d_loop_offsets, (nloops + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                             c.stream));
+    if (npairs)
+      FLN_CUDA(cudaMemcpyAsync(h_pairs.data(), d_pairs, 2 * npairs * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               c.stream));
+    FLN_CUDA(cudaStreamSynchronize(c.stream));
+    check_inputs(h_off, nloops, h_pairs);
+    const int launches = run_pairs(c, d_xyz, d_loop_offsets, h_off, h_pairs, method, prm, d_lk_out, d_err_out,
+                                   d_flags_out);
+    FLN_CUDA(cudaEventRecord(c.ev1, c.stream));
+    FLN_CUDA(cudaStreamSynchronize(c.stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+    c.stats.ms_kernels = ms;
+    c.stats.kernel_launches = launches;
+    c.stats.ms_total = now_ms() - t0;
+  });
+}
+
+fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const double *xyz2, int64_t n2,
+                           int32_t precision, double *lk_out) {
+  return guarded([&] {
+    if (!ctx || !xyz1 || !xyz2 || !lk_out || n1 < 2 || n2 < 2)
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "each loop needs at least two vertices");
+    std::vector<double> xyz(3 * (n1 + n2));
+    std::memcpy(xyz.data(), xyz1, 3 * n1 * sizeof(double));
+    std::memcpy(xyz.data() + 3 * n1, xyz2, 3 * n2 * sizeof(double));
+    const int64_t off[3] = {0, n1, n1 + n2};
+    const int32_t pr[2] = {0, 1};
+    fln_params prm;
+    fln_default_params(&prm);
+    prm.precision = precision;
+    const fln_params r = resolved(&prm);
+    compute_pairs_host(*ctx->c, xyz.data(), off, 2, pr, 1, FLN_METHOD_DIRECTSUM, r, lk_out, nullptr, nullptr);
+  });
+}
+
+fln_status fln_model_create(fln_model **out) {
+  return guarded([&] {
+    if (!out) throw Error(FLN_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = new fln_model;
+  });
+}
+void fln_model_destroy(fln_model *m) { delete m; }
+
+fln_status fln_model_load_bcc(fln_model *m, const char *path) {
+  return guarded([&] {
+    if (!m || !path) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    const std::string p(path);
+    const size_t dot = p.rfind('.');
+    std::string ext = dot == std::string::npos ? "" : p.substr(dot);
+    for (auto &ch : ext) ch = (char)std::tolower((unsigned char)ch);
+    if (ext != ".bcc") throw Error(FLN_ERR_FORMAT, "File extension for import must be .bcc: " + p);
+    load_bcc(p, m->m);
+    m->prepared_disc = -1;
+  });
+}
+
+fln_status fln_model_save_bcc(const fln_model *m, const char *path) {
+  return guarded([&] {
+    if (!m || !path) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    save_bcc(path, m->m);
+  });
+}
+
+fln_status fln_model_set_curves(fln_model *m, fln_seg_type type, int32_t ncurves, const int32_t *counts,
+                                const double *xyz) {
+  return guarded([&] {
+    if (!m || ncurves < 0 || (ncurves && !counts)) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    if ((int)type < 0 || (int)type > 3) throw Error(FLN_ERR_INVALID_ARGUMENT, "unknown segment type");
+    std::vector<CurveData> cs(ncurves);
+    int64_t at = 0;
+    for (int32_t i = 0; i < ncurves; ++i) {
+      const int64_t n = counts[i] < 0 ? -(int64_t)counts[i] : counts[i];
+      cs[i].kind = (SegKind)type;
+      cs[i].closed = counts[i] < 0;
+      cs[i].q.resize(n);
+      if (n && !xyz) throw Error(FLN_ERR_INVALID_ARGUMENT, "xyz is NULL");
+      for (int64_t k = 0; k < n; ++k, ++at) cs[i].q[k] = {xyz[3 * at], xyz[3 * at + 1], xyz[3 * at + 2]};
+    }
+    m->m.curves.swap(cs);
+    m->m.prepared = false;
+    m->prepared_disc = -1;
+  });
+}
+
+int32_t fln_model_num_curves(const fln_model *m) { return m ? (int32_t)m->m.curves.size() : 0; }
+int64_t fln_model_num_points(const fln_model *m) {
+  int64_t t = 0;
+  if (m)
+    for (auto &c : m->m.curves) t += (int64_t)c.q.size();
+  return t;
+}
+
+fln_status fln_model_get_curves(const fln_model *m, int32_t *type_out, int32_t *counts_out, double *xyz_out) {
+  return guarded([&] {
+    if (!m) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL model");
+    if (type_out) *type_out = m->m.curves.empty() ? FLN_SEG_CATMULLROM : (int32_t)m->m.curves[0].kind;
+    int64_t at = 0;
+    for (size_t i = 0; i < m->m.curves.size(); ++i) {
+      const auto &c = m->m.curves[i];
+      if (counts_out) counts_out[i] = c.closed ? -(int32_t)c.q.size() : (int32_t)c.q.size();
+      for (auto &v : c.q) {
+        if (xyz_out) {
+          xyz_out[3 * at] = v.x;
+          xyz_out[3 * at + 1] = v.y;
+          xyz_out[3 * at + 2] = v.z;
+        }
+        ++at;
+      }
+    }
+  });
+}
+
+fln_status fln_model_prepare(fln_model *m, int discretize, int32_t *rounds_out) {
+  return guarded([&] {
+    if (!m) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL model");
+    prepare(m->m, discretize != 0);
+    m->prepared_disc = discretize != 0;
+    if (rounds_out) *rounds_out = m->m.rounds;
+  });
+}
+
+fln_status fln_model_prepared_sizes(const fln_model *m, int64_t *num_vertices, int64_t *num_pairs) {
+  return guarded([&] {
+    if (!m || !m->m.prepared) throw Error(FLN_ERR_INVALID_ARGUMENT, "model not prepared");
+    if (num_vertices) *num_vertices = m->m.poly_offsets.empty() ? 0 : m->m.poly_offsets.back();
+    if (num_pairs) *num_pairs = (int64_t)m->m.pairs.size() / 2;
+  });
+}
+
+fln_status fln_model_get_prepared(const fln_model *m, int64_t *loop_offsets_out, double *xyz_out,
+                                  int32_t *pairs_out) {
+  return guarded([&] {
+    if (!m || !m->m.prepared) throw Error(FLN_ERR_INVALID_ARGUMENT, "model not prepared");
+    if (loop_offsets_out)
+      std::memcpy(loop_offsets_out, m->m.poly_offsets.data(), m->m.poly_offsets.size() * sizeof(int64_t));
+    if (xyz_out) std::memcpy(xyz_out, m->m.poly_xyz.data(), m->m.poly_xyz.size() * sizeof(double));
+    if (pairs_out) std::memcpy(pairs_out, m->m.pairs.data(), m->m.pairs.size() * sizeof(int32_t));
+  });
+}
+
+fln_status fln_certificate_compute(fln_ctx *ctx, const fln_model *model, int force_direct_sum, int discretize,
+                                   const fln_params *params, fln_certificate **out) {
+  return guarded([&] {
+    if (!ctx || !model || !out) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    const fln_params prm = resolved(params);
+    auto *mm = const_cast<fln_model *>(model);  // the prepared polylines are a cache
+    const double t0 = now_ms();
+    if (!mm->m.prepared || mm->prepared_disc != (discretize != 0)) {
+      prepare(mm->m, discretize != 0);
+      mm->prepared_disc = discretize != 0;
+    }
+    const double t1 = now_ms();
+    const Model &m = mm->m;
+    const int32_t nc = (int32_t)m.curves.size();
+    const int64_t np = (int64_t)m.pairs.size() / 2;
+    std::unique_ptr<fln_certificate> cert(new fln_certificate);
+    cert->c.pairs = m.pairs;
+    cert->c.lk.assign(np, 0.0);
+    cert->c.err.assign(np, 0.0);
+    cert->c.flags.assign(np, 0);
+    Context &c = *ctx->c;
+    if (np)
+      compute_pairs_host(c, m.poly_xyz.data(), m.poly_offsets.data(), nc, m.pairs.data(), np,
+                         force_direct_sum ? FLN_METHOD_DIRECTSUM : FLN_METHOD_BARNESHUT, prm, cert->c.lk.data(),
+                         cert->c.err.data(), cert->c.flags.data());
+    else
+      c.stats = fln_stats{};
+    fill_certificate(cert->c, nc, m.pairs, cert->c.lk);
+    c.stats.ms_discretize = t1 - t0;
+    c.stats.discretize_rounds = m.rounds;
+    c.stats.mean_off_integer = cert->c.mean_off;
+    c.stats.max_off_integer = cert->c.max_off;
+    c.stats.ms_total = now_ms() - t0;
+    *out = cert.release();
+  });
+}
+
+fln_status fln_certificate_load(const char *path, fln_certificate **out) {
+  return guarded([&] {
+    if (!path || !out) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<fln_certificate> c(new fln_certificate);
+    c->c = read_certificate(path);
+    *out = c.release();
+  });
+}
+
+void fln_certificate_destroy(fln_certificate *c) { delete c; }
+
+fln_status fln_certificate_save(const fln_certificate *c, const char *path) {
+  return guarded([&] {
+    if (!c || !path) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) throw Error(FLN_ERR_IO, std::string("Cannot write certificate: ") + path);
+    const std::string t = c->c.text();
+    const bool ok = std::fwrite(t.data(), 1, t.size(), f) == t.size();
+    std::fclose(f);
+    if (!ok) throw Error(FLN_ERR_IO, std::string("Cannot write certificate: ") + path);
+  });
+}
+
+int64_t fln_certificate_text(const fln_certificate *c, char *buf, int64_t cap) {
+  if (!c) return -1;
+  const std::string t = c->c.text();
+  if (buf && cap > 0) {
+    const int64_t k = std::min<int64_t>(cap - 1, (int64_t)t.size());
+    std::memcpy(buf, t.data(), k);
+    buf[k] = 0;
+  }
+  return (int64_t)t.size();
+}
+
+int32_t fln_certificate_num_curves(const fln_certificate *c) { return c ? c->c.ncurves : 0; }
+int64_t fln_certificate_num_entries(const fln_certificate *c) { return c ? (int64_t)c->c.entries.size() : 0; }
+
+fln_status fln_certificate_entries(const fln_certificate *c, int32_t *entries_out) {
+  return guarded([&] {
+    if (!c || !entries_out) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (size_t k = 0; k < c->c.entries.size(); ++k) {
+      entries_out[3 * k] = c->c.entries[k].i;
+      entries_out[3 * k + 1] = c->c.entries[k].j;
+      entries_out[3 * k + 2] = c->c.entries[k].lk;
+    }
+  });
+}
+
+int64_t fln_certificate_num_pairs(const fln_certificate *c) { return c ? (int64_t)c->c.lk.size() : 0; }
+
+fln_status fln_certificate_pairs(const fln_certificate *c, int32_t *pairs_out, double *lk_out, double *err_out,
+                                 int32_t *flags_out) {
+  return guarded([&] {
+    if (!c) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL certificate");
+    const size_t np = c->c.lk.size();
+    if (pairs_out) std::memcpy(pairs_out, c->c.pairs.data(), 2 * np * sizeof(int32_t));
+    if (lk_out) std::memcpy(lk_out, c->c.lk.data(), np * sizeof(double));
+    if (err_out) std::memcpy(err_out, c->c.err.data(), np * sizeof(double));
+    if (flags_out) std::memcpy(flags_out, c->c.flags.data(), np * sizeof(int32_t));
+  });
+}
+
+int fln_certificate_equals(const fln_certificate *a, const fln_certificate *b) {
+  if (!a || !b || a->c.ncurves != b->c.ncurves || a->c.entries.size() != b->c.entries.size()) return 0;
+  for (size_t k = 0; k < a->c.entries.size(); ++k) {
+    const auto &x = a->c.entries[k], &y = b->c.entries[k];
+    if (x.i != y.i || x.j != y.j || x.lk != y.lk) return 0;
+  }
+  return 1;
+}
+
+fln_status fln_certificate_export_diffs(const fln_certificate *self, const fln_certificate *other,
+                                        const char *diff_pairs_path, const char *diff_curves_path) {
+  return guarded([&] {
+    if (!self || !other) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL certificate");
+    export_diffs(self->c, other->c, diff_pairs_path ? diff_pairs_path : "", diff_curves_path ? diff_curves_path : "");
+  });
+}
+
+}  // extern "C"

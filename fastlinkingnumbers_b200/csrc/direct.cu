@@ -1,0 +1,361 @@
+// Direct summation of the Gauss linking integral on B200 (sm_100a).
+//
+// Work: every potential loop pair (i, j) is split into items of kBlockSegs
+// consecutive segments of its longer loop ("curve 1"); one CTA of kBlockSegs
+// threads takes items from a device work queue (an atomic counter) until it
+// runs dry, so all pairs — 16-segment rings to 2^18-segment loops — run in
+// one persistent launch. Each thread owns one curve-1 segment and walks all
+// curve-2 segments, which the CTA stages tile by tile in shared memory
+// (coalesced loads, broadcast reads). Per segment pair it evaluates the
+// closed-form solid-angle term of Arai 2013 as the reference does
+// (src/compute_link.cpp:126-178, :200-280): with a = q_k - p_i,
+// b = q_k - p_{i+1}, c = q_{k+1} - p_{i+1}, d = q_{k+1} - p_i,
+//   det  = a . (b x c)
+//   div1 = |a||b||c| + (a.b)|c| + (c.a)|b| + (c.b)|a|
+//   div2 = |a||d||c| + (a.d)|c| + (c.a)|d| + (c.d)|a|
+//   term = atan2(det (div1 + div2), div1 div2 - det^2) / 2pi
+//          + [det (div1 + div2) det < 0] sign(det)          (in full turns).
+// Consecutive steps share vertices: step k+1's a, b are step k's d, c, so
+// each step computes two new difference vectors and two norms.
+//
+// Two precisions:
+//  * FP64 ("plain FP64 GPU direct sum"): every operation in FP64; the per-
+//    thread terms are combined by the arctangent-addition recurrence of
+//    ComputeLinkingNumberDirectFast (Bertolazzi et al. 2019) — a running
+//    complex product with a count of negative-x-axis crossings — and one
+//    atan2 per thread per item. The product is rescaled by an exact power of
+//    two each step instead of the reference's division.
+//  * MIXED: coordinates relative to the tile's first vertex in FP32, one
+//    FP32 atan2 per segment pair, FP32 sums over one tile of kTile terms and
+//    FP64 sums above that. det uses the identity det = a . (f x e) with
+//    e = p_{i+1} - p_i and f = q_{k+1} - q_k, which keeps its relative
+//    accuracy for distant pairs. A segment pair whose closest endpoint
+//    distance is below near_factor x (longer segment length) is recomputed
+//    in FP64 (near-singular terms).
+// Item results go to one FP64 partial per item; a second kernel sums them
+// per pair in a fixed order, so results are deterministic.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "engine.hpp"
+
+namespace fln {
+namespace {
+
+constexpr int kBlockSegs = 128;  // threads per CTA = curve-1 segments per item
+constexpr int kTile = 256;       // curve-2 vertices per shared-memory tile
+constexpr double kInvTwoPi = 0.15915494309189533576888376337251436;
+
+struct DirectArgs {
+  const double *xyz;          // 3 doubles per vertex
+  const int64_t *off;         // loop offsets
+  const int32_t *loops;       // per slot: (curve-1 loop, curve-2 loop)
+  const int64_t *item_start;  // per slot: first item; nslots + 1 entries
+  int32_t nslots;
+  int64_t items;
+  double *partial;                   // per item
+  unsigned long long *counter;       // [0] work queue head, [1] near-term count
+  float near_factor;
+};
+
+__device__ __forceinline__ int find_slot(const int64_t *start, int n, int64_t item) {
+  int lo = 0, hi = n;  // start[lo] <= item < start[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(start + mid) <= item) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ double3 load_v(const double *xyz, int64_t v) {
+  return make_double3(__ldg(xyz + 3 * v), __ldg(xyz + 3 * v + 1), __ldg(xyz + 3 * v + 2));
+}
+
+// Sum over the CTA; the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double *s_red) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_red[warp] = v;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kBlockSegs / 32; ++w) r += s_red[w];
+  return r;
+}
+
+// One segment pair in FP64, in full turns (OneArctanPerPair form,
+// compute_link.cpp:151-175 divided by 4 pi).
+__device__ __noinline__ double term_fp64(double3 p0, double3 p1, double3 q0, double3 q1) {
+  const double ax = q0.x - p0.x, ay = q0.y - p0.y, az = q0.z - p0.z;
+  const double bx = q0.x - p1.x, by = q0.y - p1.y, bz = q0.z - p1.z;
+  const double cx = q1.x - p1.x, cy = q1.y - p1.y, cz = q1.z - p1.z;
+  const double dx = q1.x - p0.x, dy = q1.y - p0.y, dz = q1.z - p0.z;
+  const double la = sqrt(ax * ax + ay * ay + az * az), lb = sqrt(bx * bx + by * by + bz * bz);
+  const double lc = sqrt(cx * cx + cy * cy + cz * cz), ld = sqrt(dx * dx + dy * dy + dz * dz);
+  const double ca = cx * ax + cy * ay + cz * az;
+  const double div1 = la * lb * lc + (ax * bx + ay * by + az * bz) * lc + ca * lb + (cx * bx + cy * by + cz * bz) * la;
+  const double div2 = la * ld * lc + (ax * dx + ay * dy + az * dz) * lc + ca * ld + (cx * dx + cy * dy + cz * dz) * la;
+  const double det = ax * (by * cz - bz * cy) + az * (bx * cy - by * cx) + ay * (bz * cx - bx * cz);
+  const double xp = div1 * div2 - det * det, yp = det * (div1 + div2);
+  double r = atan2(yp, xp) * kInvTwoPi;
+  if (yp * det < 0) r += (det > 0) ? 1.0 : -1.0;
+  return r;
+}
+
+// Rescales (x, y) by the power of two that brings max(|x|, |y|) into [1, 2).
+__device__ __forceinline__ void renorm(double &x, double &y) {
+  const double m = fmax(fabs(x), fabs(y));
+  int e = (__double2hiint(m) >> 20) & 0x7ff;
+  e = min(max(e, 1), 2045);
+  const double s = __hiloint2double((2046 - e) << 20, 0);
+  x *= s;
+  y *= s;
+}
+
+// ------------------------------------------------------------------ FP64
+__global__ void __launch_bounds__(kBlockSegs) direct_fp64_kernel(DirectArgs A) {
+  __shared__ double sx[kTile + 1], sy[kTile + 1], sz[kTile + 1];
+  __shared__ double s_red[kBlockSegs / 32];
+  __shared__ long long s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(A.counter, 1ULL);
+    __syncthreads();
+    const int64_t item = s_item;
+    if (item >= A.items) break;
+    const int slot = find_slot(A.item_start, A.nslots, item);
+    const int64_t blk = item - A.item_start[slot];
+    const int l1 = A.loops[2 * slot], l2 = A.loops[2 * slot + 1];
+    const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1;
+    const int64_t o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
+    const int64_t i = blk * kBlockSegs + threadIdx.x;
+    const bool active = i < n1;
+    double3 p0 = make_double3(0, 0, 0), p1 = p0;
+    if (active) {
+      p0 = load_v(A.xyz, o1 + i);
+      p1 = load_v(A.xyz, o1 + (i + 1 == n1 ? 0 : i + 1));
+    }
+    double xs = 1.0, ys = 0.0, S = -1.0, turns = 0.0;
+    for (int64_t k0 = 0; k0 < n2; k0 += kTile) {
+      const int kt = (int)(n2 - k0 < kTile ? n2 - k0 : kTile);
+      __syncthreads();
+      for (int t = threadIdx.x; t <= kt; t += kBlockSegs) {
+        const int64_t kk = k0 + t;
+        const double3 v = load_v(A.xyz, o2 + (kk == n2 ? 0 : kk));
+        sx[t] = v.x;
+        sy[t] = v.y;
+        sz[t] = v.z;
+      }
+      __syncthreads();
+      if (!active) continue;
+      double ax = sx[0] - p0.x, ay = sy[0] - p0.y, az = sz[0] - p0.z;
+      double bx = sx[0] - p1.x, by = sy[0] - p1.y, bz = sz[0] - p1.z;
+      double la = sqrt(ax * ax + ay * ay + az * az), lb = sqrt(bx * bx + by * by + bz * bz);
+      double ab = ax * bx + ay * by + az * bz;
+      for (int k = 0; k < kt; ++k) {
+        const double qx = sx[k + 1], qy = sy[k + 1], qz = sz[k + 1];
+        const double cx = qx - p1.x, cy = qy - p1.y, cz = qz - p1.z;
+        const double dx = qx - p0.x, dy = qy - p0.y, dz = qz - p0.z;
+        const double lc = sqrt(cx * cx + cy * cy + cz * cz), ld = sqrt(dx * dx + dy * dy + dz * dz);
+        const double ca = cx * ax + cy * ay + cz * az;
+        const double cb = cx * bx + cy * by + cz * bz;
+        const double ad = ax * dx + ay * dy + az * dz;
+        const double cd = cx * dx + cy * dy + cz * dz;
+        const double det = ax * (by * cz - bz * cy) + az * (bx * cy - by * cx) + ay * (bz * cx - bx * cz);
+        const double t = la * lc;
+        const double div1 = t * lb + ab * lc + ca * lb + cb * la;
+        const double div2 = t * ld + ad * lc + ca * ld + cd * la;
+        const double xp = div1 * div2 - det * det;
+        const double yp = det * (div1 + div2);
+        // Arctangent addition: (xs + i ys) *= (xp + i yp), tracking crossings
+        // of the negative real axis (compute_link.cpp:245-269).
+        double ny = xs * yp + xp * ys;
+        double nx = xs * xp - ys * yp;
+        renorm(nx, ny);
+        if (yp * det < 0) turns += (det > 0) ? 1.0 : -1.0;
+        const double s3 = (ny > 0.0 || (ny == 0.0 && nx < 0.0)) ? 1.0 : -1.0;
+        if (s3 * S < 0 && yp * S >= 0) turns += S;
+        xs = nx;
+        ys = ny;
+        S = s3;
+        ax = dx; ay = dy; az = dz;
+        bx = cx; by = cy; bz = cz;
+        la = ld; lb = lc; ab = cd;
+      }
+    }
+    const double v = active ? atan2(ys, xs) * kInvTwoPi + turns : 0.0;
+    const double s = block_sum(v, s_red);
+    if (threadIdx.x == 0) A.partial[item] = s;
+  }
+}
+
+// ------------------------------------------------------------------ mixed
+__global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) {
+  __shared__ float4 sq[kTile + 1];  // xyz relative to the tile origin; w = length of segment t
+  __shared__ double s_red[kBlockSegs / 32];
+  __shared__ long long s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(A.counter, 1ULL);
+    __syncthreads();
+    const int64_t item = s_item;
+    if (item >= A.items) break;
+    const int slot = find_slot(A.item_start, A.nslots, item);
+    const int64_t blk = item - A.item_start[slot];
+    const int l1 = A.loops[2 * slot], l2 = A.loops[2 * slot + 1];
+    const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1;
+    const int64_t o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
+    const int64_t i = blk * kBlockSegs + threadIdx.x;
+    const bool active = i < n1;
+    double3 p0 = make_double3(0, 0, 0), p1 = p0;
+    if (active) {
+      p0 = load_v(A.xyz, o1 + i);
+      p1 = load_v(A.xyz, o1 + (i + 1 == n1 ? 0 : i + 1));
+    }
+    const float ex = (float)(p1.x - p0.x), ey = (float)(p1.y - p0.y), ez = (float)(p1.z - p0.z);
+    const float len1 = sqrtf(ex * ex + ey * ey + ez * ez);
+    double acc = 0.0, near_turns = 0.0;
+    int turns = 0;
+    unsigned near_count = 0;
+    for (int64_t k0 = 0; k0 < n2; k0 += kTile) {
+      const int kt = (int)(n2 - k0 < kTile ? n2 - k0 : kTile);
+      const double3 O = load_v(A.xyz, o2 + k0);
+      __syncthreads();
+      for (int t = threadIdx.x; t <= kt; t += kBlockSegs) {
+        const int64_t kk = k0 + t;
+        const double3 v = load_v(A.xyz, o2 + (kk == n2 ? 0 : kk));
+        sq[t] = make_float4((float)(v.x - O.x), (float)(v.y - O.y), (float)(v.z - O.z), 0.f);
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < kt; t += kBlockSegs) {
+        const float4 a = sq[t], b = sq[t + 1];
+        const float fx = b.x - a.x, fy = b.y - a.y, fz = b.z - a.z;
+        sq[t].w = sqrtf(fx * fx + fy * fy + fz * fz);
+      }
+      __syncthreads();
+      if (!active) continue;
+      const float r0x = (float)(p0.x - O.x), r0y = (float)(p0.y - O.y), r0z = (float)(p0.z - O.z);
+      const float r1x = (float)(p1.x - O.x), r1y = (float)(p1.y - O.y), r1z = (float)(p1.z - O.z);
+      float4 q = sq[0];
+      float ax = q.x - r0x, ay = q.y - r0y, az = q.z - r0z;
+      float bx = q.x - r1x, by = q.y - r1y, bz = q.z - r1z;
+      float la = sqrtf(ax * ax + ay * ay + az * az), lb = sqrtf(bx * bx + by * by + bz * bz);
+      float ab = ax * bx + ay * by + az * bz;
+      float accf = 0.f;
+      for (int k = 0; k < kt; ++k) {
+        const float4 qn = sq[k + 1];
+        const float cx = qn.x - r1x, cy = qn.y - r1y, cz = qn.z - r1z;
+        const float dx = qn.x - r0x, dy = qn.y - r0y, dz = qn.z - r0z;
+        const float lc = sqrtf(cx * cx + cy * cy + cz * cz), ld = sqrtf(dx * dx + dy * dy + dz * dz);
+        const float cd = cx * dx + cy * dy + cz * dz;
+        const float close = fminf(fminf(la, lb), fminf(lc, ld));
+        if (close < A.near_factor * fmaxf(len1, q.w)) {
+          const int64_t kk = k0 + k, kn = kk + 1;
+          near_turns += term_fp64(p0, p1, load_v(A.xyz, o2 + kk), load_v(A.xyz, o2 + (kn == n2 ? 0 : kn)));
+          ++near_count;
+        } else {
+          const float ca = cx * ax + cy * ay + cz * az;
+          const float cb = cx * bx + cy * by + cz * bz;
+          const float ad = ax * dx + ay * dy + az * dz;
+          const float fx = qn.x - q.x, fy = qn.y - q.y, fz = qn.z - q.z;
+          const float det = ax * (fy * ez - fz * ey) + ay * (fz * ex - fx * ez) + az * (fx * ey - fy * ex);
+          const float t = la * lc;
+          const float div1 = t * lb + ab * lc + ca * lb + cb * la;
+          const float div2 = t * ld + ad * lc + ca * ld + cd * la;
+          const float xp = div1 * div2 - det * det;
+          const float yp = det * (div1 + div2);
+          accf += atan2f(yp, xp);
+          if (yp * det < 0.f) turns += (det > 0.f) ? 1 : -1;
+        }
+        q = qn;
+        ax = dx; ay = dy; az = dz;
+        bx = cx; by = cy; bz = cz;
+        la = ld; lb = lc; ab = cd;
+      }
+      acc += (double)accf;
+    }
+    const double v = active ? acc * kInvTwoPi + (double)turns + near_turns : 0.0;
+    const double s = block_sum(v, s_red);
+    if (threadIdx.x == 0) A.partial[item] = s;
+    if (near_count) atomicAdd(A.counter + 1, (unsigned long long)near_count);
+  }
+}
+
+// Sums the item partials of each slot in item order and scatters the result
+// to the caller's pair index.
+__global__ void reduce_items_kernel(const double *partial, const int64_t *item_start, const int32_t *order,
+                                    int32_t nslots, double *lk_out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  double acc = 0.0;
+  for (int64_t it = item_start[s]; it < item_start[s + 1]; ++it) acc += partial[it];
+  lk_out[order[s]] = acc;
+}
+
+}  // namespace
+
+int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
+                      const std::vector<int32_t> &h_pairs, int precision, double near_factor, double *d_lk_out,
+                      double *near_terms_out) {
+  const int64_t np = (int64_t)h_pairs.size() / 2;
+  if (np == 0) return 0;
+  // Plan: orient each pair so its longer loop is curve 1, and order slots by
+  // decreasing work so the queue hands out the largest pairs first.
+  std::vector<int32_t> order(np);
+  std::iota(order.begin(), order.end(), 0);
+  auto nseg = [&](int l) { return h_off[l + 1] - h_off[l]; };
+  std::vector<double> cost(np);
+  for (int64_t p = 0; p < np; ++p) cost[p] = (double)nseg(h_pairs[2 * p]) * (double)nseg(h_pairs[2 * p + 1]);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<int32_t> loops(2 * np);
+  std::vector<int64_t> start(np + 1);
+  start[0] = 0;
+  for (int64_t s = 0; s < np; ++s) {
+    int a = h_pairs[2 * order[s]], b = h_pairs[2 * order[s] + 1];
+    if (nseg(b) > nseg(a)) std::swap(a, b);
+    loops[2 * s] = a;
+    loops[2 * s + 1] = b;
+    start[s + 1] = start[s] + (nseg(a) + kBlockSegs - 1) / kBlockSegs;
+  }
+  const int64_t items = start[np];
+  int32_t *d_loops = ctx.d_loops.as<int32_t>(2 * np + np);
+  int32_t *d_order = d_loops + 2 * np;
+  int64_t *d_start = ctx.d_items.as<int64_t>(np + 1);
+  double *d_partial = ctx.d_partial.as<double>(items);
+  unsigned long long *d_counter = ctx.d_counter.as<unsigned long long>(2);
+  FLN_CUDA(cudaMemcpyAsync(d_loops, loops.data(), 2 * np * sizeof(int32_t), cudaMemcpyHostToDevice, ctx.stream));
+  FLN_CUDA(cudaMemcpyAsync(d_order, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, ctx.stream));
+  FLN_CUDA(cudaMemcpyAsync(d_start, start.data(), (np + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+  FLN_CUDA(cudaMemsetAsync(d_counter, 0, 2 * sizeof(unsigned long long), ctx.stream));
+  DirectArgs A{d_xyz, d_off, d_loops, d_start, (int32_t)np, items, d_partial, d_counter, (float)near_factor};
+  int per_sm = 0;
+  FLN_CUDA(cudaEventRecord(ctx.ev2, ctx.stream));
+  if (precision == FLN_PREC_FP64) {
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel, kBlockSegs, 0));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)ctx.num_sms * std::max(per_sm, 1)));
+    direct_fp64_kernel<<<grid, kBlockSegs, 0, ctx.stream>>>(A);
+  } else {
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel, kBlockSegs, 0));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)ctx.num_sms * std::max(per_sm, 1)));
+    direct_mixed_kernel<<<grid, kBlockSegs, 0, ctx.stream>>>(A);
+  }
+  FLN_CUDA(cudaGetLastError());
+  FLN_CUDA(cudaEventRecord(ctx.ev3, ctx.stream));
+  reduce_items_kernel<<<(int)((np + 255) / 256), 256, 0, ctx.stream>>>(d_partial, d_start, d_order, (int32_t)np,
+                                                                      d_lk_out);
+  FLN_CUDA(cudaGetLastError());
+  if (near_terms_out) {
+    unsigned long long h = 0;
+    FLN_CUDA(cudaMemcpyAsync(&h, d_counter + 1, sizeof h, cudaMemcpyDeviceToHost, ctx.stream));
+    FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+    *near_terms_out = (double)h;
+  }
+  ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+  return 2;
+}
+
+}  // namespace fln

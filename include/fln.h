@@ -1,0 +1,204 @@
+/*
+ * fln.h — C ABI of the B200 linking-number engine (libfln.so).
+ *
+ * This is the drop-in boundary for the hot path of antequ/fastlinkingnumbers
+ * (`verifycurves`): the Gauss linking integral over every potentially linked
+ * loop pair, by direct summation or two-tree Barnes–Hut, plus the host stages
+ * that feed it (BCC loading, potential-link search, Discretize) and the
+ * certificate built from it. Plain C types only: pointers, sizes, enums.
+ * Every entry point returns an fln_status and never throws; on failure
+ * fln_last_error() describes the cause (thread-local).
+ *
+ * Each declaration names the reference interface (file:line in
+ * antequ/fastlinkingnumbers) it replaces.
+ */
+#ifndef FLN_H_
+#define FLN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLN_ABI_VERSION 1
+
+typedef enum fln_status {
+  FLN_OK = 0,
+  FLN_ERR_INVALID_ARGUMENT = 1,
+  FLN_ERR_IO = 2,              /* file open / short read / write (model.cpp:284-356) */
+  FLN_ERR_FORMAT = 3,          /* bad BCC header, type or counts (model.cpp:294-328) */
+  FLN_ERR_CUDA = 4,            /* a CUDA runtime call failed */
+  FLN_ERR_NO_DEVICE = 5,       /* no CUDA device visible */
+  FLN_ERR_OUT_OF_MEMORY = 6,
+  FLN_ERR_SEGMENT_TOO_SMALL = 7, /* Discretize: piece < eps * avg coordinate (discretize.cpp:151-160, 219-229) */
+  FLN_ERR_MAX_RECURSION = 8,   /* Discretize: more than 55 rounds (discretize.cpp:248-253) */
+  FLN_ERR_UNLOOPED = 9,        /* an open curve reached the linking-number stage (curve.cpp:126-128) */
+  FLN_ERR_NONFINITE = 10,      /* a pair stayed NaN/inf after the FP64 recompute (lnc.cpp:206-211) */
+  FLN_ERR_STACK_OVERFLOW = 11, /* a Barnes–Hut traversal stack exceeded its bound */
+  FLN_ERR_TIMEOUT = 12,        /* a bounded device wait ran out */
+  FLN_ERR_INTERNAL = 13
+} fln_status;
+
+typedef enum fln_method {
+  FLN_METHOD_DIRECTSUM = 0, /* --method directsum  (lnc.cpp:241-338) */
+  FLN_METHOD_BARNESHUT = 1  /* --method barneshut  (lnc.cpp:102-229) */
+} fln_method;
+
+typedef enum fln_precision {
+  FLN_PREC_FP64 = 0,  /* every term in FP64: the plain FP64 GPU path */
+  FLN_PREC_MIXED = 1  /* FP32 terms, FP64 near-singular terms and per-pair sums, FP64 recompute below margin */
+} fln_precision;
+
+typedef enum fln_seg_type {
+  FLN_SEG_BSPLINE = 0,    /* BCC "BS" (curve.cpp:20-29) */
+  FLN_SEG_CATMULLROM = 1, /* BCC "C0" (curve.cpp:31-36) */
+  FLN_SEG_BEZIER = 2,     /* BCC "BZ" (curve.cpp:38-43) */
+  FLN_SEG_POLYLINE = 3    /* BCC "PL" */
+} fln_seg_type;
+
+/* Per-pair result flags (bit set). */
+enum {
+  FLN_PAIR_FP64_RECOMPUTED = 1, /* margin below threshold or non-finite: recomputed in FP64 direct sum */
+  FLN_PAIR_BETA_RETRIED = 2,    /* Barnes–Hut re-run with the larger beta (lnc.cpp:165-184) */
+  FLN_PAIR_NONFINITE = 4,       /* still non-finite after the recompute */
+  FLN_PAIR_SWAPPED = 8          /* evaluated with the loops' roles exchanged (symmetric) */
+};
+
+typedef struct fln_params {
+  double barnes_hut_init_beta;  /* 2.0  (define_args.h:50-51) */
+  double barnes_hut_beta_limit; /* 10.0 (define_args.h:53-54) */
+  double epssq;                 /* 1e-24 CERTIFICATE_EPSSQ (lnc.cpp:24) */
+  double target_error;          /* 0.1   TARGET_ERROR (lnc.cpp:25) */
+  double error_est_scale;       /* 0.05  ERROR_EST_SCALE (lnc.cpp:26) */
+  int32_t precision;            /* fln_precision; default FLN_PREC_MIXED */
+  double fp64_margin;           /* recompute in FP64 when 0.5 - |lk - round(lk)| < this; default 0.25 */
+  double near_factor;           /* mixed direct sum: a segment pair whose closest endpoint distance is
+                                   below near_factor * (longer segment length) is evaluated in FP64; 1.0 */
+  int32_t bh_tree;              /* Barnes–Hut tree: 0 = curve-order tree (default), 1 = the reference's
+                                   kd-median tree (ModifiedKdBVH.h:207-237) */
+  int32_t reserved[7];
+} fln_params;
+
+/* Statistics of the last computation on a context. */
+typedef struct fln_stats {
+  int64_t pairs;                /* loop pairs evaluated */
+  double segment_pairs;         /* sum over pairs of n_i * n_j (direct-sum-equivalent work) */
+  int64_t fp64_recomputed;      /* pairs recomputed in FP64 */
+  int64_t beta_retried;         /* Barnes–Hut pairs re-run with a larger beta */
+  double bh_far_evals;          /* Barnes–Hut far-field node pairs evaluated */
+  double bh_leaf_evals;         /* Barnes–Hut leaf-leaf segment pairs evaluated */
+  double near_fp64_terms;       /* mixed direct sum: segment pairs evaluated in FP64 */
+  double ms_kernels;            /* device time of the linking-number kernels (CUDA events) */
+  double ms_total;              /* wall time of the last call */
+  double ms_discretize;         /* host Discretize + potential-link search (certificate calls) */
+  double mean_off_integer, max_off_integer; /* lnc.cpp:216-225 */
+  int32_t discretize_rounds;
+  int32_t kernel_launches;      /* kernels launched by the last call */
+  double ms_main_kernel;        /* device time of the dominant kernel(s): the Barnes–Hut traversal or the
+                                   direct-sum kernel (CUDA events on the launching stream) */
+  double ms_tree_build;         /* Barnes–Hut tree topology + FP64 moment build */
+} fln_stats;
+
+typedef struct fln_ctx fln_ctx;
+typedef struct fln_model fln_model;
+typedef struct fln_certificate fln_certificate;
+
+const char *fln_status_string(fln_status s);
+const char *fln_last_error(void);
+int fln_abi_version(void);
+void fln_default_params(fln_params *p);
+
+/* Context: one CUDA device and one stream; owns all device buffers.
+ * stream = 0 creates a private stream; otherwise the given cudaStream_t
+ * (as an opaque pointer) is used and not destroyed. */
+fln_status fln_ctx_create(int device, void *stream, fln_ctx **out);
+void fln_ctx_destroy(fln_ctx *ctx);
+fln_status fln_ctx_stats(const fln_ctx *ctx, fln_stats *out);
+
+/* ---- Kernel-level batched API: replaces the per-pair calls of
+ * compute_link.h:62-87 (ComputeLinkingNumberDirectOneArctanPerPair,
+ * ComputeLinkingNumberDirectFast) and :95-181 (MakeSegmentTrees,
+ * BuildTreeMoments, EvalLinkingNumberBarnesHut) with the per-pair driver
+ * loops of linking_number_certificate.cpp:102-229 and :241-338.
+ *
+ * Closed polylines: loop l owns vertices [loop_offsets[l], loop_offsets[l+1])
+ * of xyz (3 doubles per vertex); segment k runs from vertex k to k+1 (mod n).
+ * pairs holds npairs (i, j) loop-index pairs. Outputs (any may be NULL
+ * except lk_out): lk_out[p] the real-valued linking number, err_out[p] the
+ * Barnes–Hut error estimate after ERROR_EST_SCALE (0 for direct sum),
+ * flags_out[p] FLN_PAIR_* bits. Host pointers; copies are done inside. */
+fln_status fln_linking_numbers(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets,
+                               int32_t nloops, const int32_t *pairs, int64_t npairs,
+                               fln_method method, const fln_params *params, double *lk_out,
+                               double *err_out, int32_t *flags_out);
+
+/* The same with every array already in device memory (the ctx's device). */
+fln_status fln_linking_numbers_device(fln_ctx *ctx, const double *d_xyz,
+                                      const int64_t *d_loop_offsets, int32_t nloops,
+                                      const int32_t *d_pairs, int64_t npairs, fln_method method,
+                                      const fln_params *params, double *d_lk_out,
+                                      double *d_err_out, int32_t *d_flags_out);
+
+/* One pair, host arrays (compute_link.h:62-64 and :86-87). */
+fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const double *xyz2,
+                           int64_t n2, int32_t precision, double *lk_out);
+
+/* ---- Models (model.h:24-75, curve.h:41-195) */
+fln_status fln_model_create(fln_model **out);
+void fln_model_destroy(fln_model *m);
+/* Model::ImportFromFile / ImportBccFile (model.cpp:44-54, :280-364). */
+fln_status fln_model_load_bcc(fln_model *m, const char *path);
+/* Model::ExportToFile / ExportBccFile (model.cpp:61-71, :367-452). */
+fln_status fln_model_save_bcc(const fln_model *m, const char *path);
+/* Replace the curves: counts[c] control points (negative = closed loop, the
+ * BCC convention), xyz packed 3 doubles per point, one segment type. */
+fln_status fln_model_set_curves(fln_model *m, fln_seg_type type, int32_t ncurves,
+                                const int32_t *counts, const double *xyz);
+int32_t fln_model_num_curves(const fln_model *m);
+int64_t fln_model_num_points(const fln_model *m);
+/* counts_out[ncurves] (negative = loop), xyz_out[3 * num_points]. */
+fln_status fln_model_get_curves(const fln_model *m, int32_t *type_out, int32_t *counts_out,
+                                double *xyz_out);
+
+/* ---- Host stages feeding the kernels.
+ * PotentialLinkSearch + Discretize + unique PLS (lnc.cpp:61-83;
+ * discretize.cpp:103-281; potential_link_search.cpp:88-165): writes the
+ * discretized closed polylines and the sorted unique (i < j) pairs into
+ * buffers owned by the model (read them with fln_model_get_prepared). */
+fln_status fln_model_prepare(fln_model *m, int discretize, int32_t *rounds_out);
+fln_status fln_model_prepared_sizes(const fln_model *m, int64_t *num_vertices, int64_t *num_pairs);
+fln_status fln_model_get_prepared(const fln_model *m, int64_t *loop_offsets_out, double *xyz_out,
+                                  int32_t *pairs_out);
+
+/* ---- Certificates (linking_number_certificate.h:25-131) */
+/* LinkingNumberCertificate::ComputeFromModel (lnc.cpp:358-394). */
+fln_status fln_certificate_compute(fln_ctx *ctx, const fln_model *m, int force_direct_sum,
+                                   int discretize, const fln_params *params,
+                                   fln_certificate **out);
+/* LinkingNumberCertificate(filename) / ImportFromFile / ReadMatrix (lnc.cpp:43-46, :402-430). */
+fln_status fln_certificate_load(const char *path, fln_certificate **out);
+void fln_certificate_destroy(fln_certificate *c);
+/* ExportToFile / SaveMatrix (lnc.cpp:441-454, :484-486). */
+fln_status fln_certificate_save(const fln_certificate *c, const char *path);
+/* The certificate text; returns its length (writes at most cap-1 bytes + NUL when buf != NULL). */
+int64_t fln_certificate_text(const fln_certificate *c, char *buf, int64_t cap);
+int32_t fln_certificate_num_curves(const fln_certificate *c);
+int64_t fln_certificate_num_entries(const fln_certificate *c);
+/* entries_out[3 * k] = (i, j, lk) with i < j, sorted by (i, j). */
+fln_status fln_certificate_entries(const fln_certificate *c, int32_t *entries_out);
+/* Per potential pair of the last compute: (i, j), real sum, error estimate, flags. */
+int64_t fln_certificate_num_pairs(const fln_certificate *c);
+fln_status fln_certificate_pairs(const fln_certificate *c, int32_t *pairs_out, double *lk_out,
+                                 double *err_out, int32_t *flags_out);
+/* Equals / operator== (linking_number_certificate.h:117-128): 1 if equal. */
+int fln_certificate_equals(const fln_certificate *a, const fln_certificate *b);
+/* ExportDiffsToFiles (lnc.cpp:520-561); a NULL path or "[none]" skips that file. */
+fln_status fln_certificate_export_diffs(const fln_certificate *self, const fln_certificate *other,
+                                        const char *diff_pairs_path, const char *diff_curves_path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLN_H_ */
