@@ -50,12 +50,13 @@ def _peaks():
         return PEAKS_FALLBACK, "fallback"
 
 
-def make_workload(name: str, seed: int):
+def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000):
     from fastlinkingnumbers_b200 import Model, workloads as W
     if name == "polymer":
-        off, xyz = W.polymer(seed=seed)
-        cfg = {"workload": "polymer loops: 200 x 50,000-step closed Gaussian walks (10M segments), cube 400",
-               "loops": 200, "steps_per_loop": 50000}
+        off, xyz = W.polymer(seed=seed, n_loops=loops, n_steps=steps)
+        cfg = {"workload": f"polymer loops: {loops} x {steps}-step closed Gaussian walks "
+                           f"({loops * steps / 1e6:g}M segments), cube 400",
+               "loops": loops, "steps_per_loop": steps}
     elif name == "chain_mail":
         off, xyz = W.chain_mail(seed=seed)
         cfg = {"workload": "chain-mail sheet: 100 x 100 rings, 48-gons (480k segments)", "loops": 10000}
@@ -144,7 +145,7 @@ def cpu_sample_run(poff, pxyz, pairs, target_s: float, seed: int, nthreads: int)
 def run_reference(args, rank):
     if rank != 0:
         return
-    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed)
+    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed, args.loops, args.loop_steps)
     from oracle import pyoracle
     threads = pyoracle.max_threads()
     vals = []
@@ -176,7 +177,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank)
+    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank, args.loops, args.loop_steps)
     stream = torch.cuda.current_stream()
     eng = Engine(local_rank, stream.cuda_stream)
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
@@ -197,8 +198,13 @@ def run_ours(args, rank, world, local_rank):
                                    d_flags.data_ptr(), method=args.method, params=prm)
         return eng.stats()
 
-    for _ in range(args.warmup):
-        step()
+    for w in range(args.warmup):
+        t0 = time.perf_counter()
+        s = step()
+        print(f"[bench] warmup {w}: {1e3 * (time.perf_counter() - t0):.1f} ms wall, main kernel "
+              f"{s['ms_main_kernel']:.1f} ms, tree {s['ms_tree_build']:.1f} ms, far {s['bh_far_evals']:.3g}, "
+              f"leaf {s['bh_leaf_evals']:.3g}, retried {s['beta_retried']}, fp64 {s['fp64_recomputed']}",
+              file=sys.stderr, flush=True)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -317,6 +323,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--bh-tree", type=int, default=0)
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--loops", type=int, default=200)
+    ap.add_argument("--loop-steps", type=int, default=50000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
     ap.add_argument("--traffic-bytes", type=float, default=None)

@@ -26,6 +26,7 @@ METHOD_DIRECTSUM, METHOD_BARNESHUT = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 SEG_BSPLINE, SEG_CATMULLROM, SEG_BEZIER, SEG_POLYLINE = 0, 1, 2, 3
 PAIR_FP64_RECOMPUTED, PAIR_BETA_RETRIED, PAIR_NONFINITE, PAIR_SWAPPED = 1, 2, 4, 8
+PAIR_BETA_ESCALATED = 16
 
 # Every symbol include/fln.h declares (checked by the CPU tests).
 EXPORTED = [
@@ -47,7 +48,8 @@ class Params(C.Structure):
         ("barnes_hut_init_beta", C.c_double), ("barnes_hut_beta_limit", C.c_double),
         ("epssq", C.c_double), ("target_error", C.c_double), ("error_est_scale", C.c_double),
         ("precision", C.c_int32), ("fp64_margin", C.c_double), ("near_factor", C.c_double),
-        ("bh_tree", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -59,7 +61,8 @@ class Stats(C.Structure):
         ("ms_discretize", C.c_double), ("mean_off_integer", C.c_double),
         ("max_off_integer", C.c_double), ("discretize_rounds", C.c_int32),
         ("kernel_launches", C.c_int32), ("ms_main_kernel", C.c_double),
-        ("ms_tree_build", C.c_double),
+        ("ms_tree_build", C.c_double), ("bh_rounds", C.c_int32), ("reserved_stats", C.c_int32),
+        ("bh_escalated", C.c_int64),
     ]
 
     def as_dict(self):

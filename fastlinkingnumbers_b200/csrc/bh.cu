@@ -35,6 +35,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <numeric>
 
@@ -253,25 +254,42 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
 }
 
 // ------------------------------------------------------------------ traversal
+// A unit of traversal work: up to 32 node pairs of one loop pair (slot).
+struct Batch {
+  int32_t slot;
+  int32_t count;
+  int2 pairs[32];
+};
+
 struct TravArgs {
   const double *xyz;
   const int64_t *off;
   const int64_t *node_base;
   const NodeHdr *hdr;
   const NodeMom *mom;
-  const int32_t *slot_loops;  // 2 per slot
-  const int32_t *slot_pair;   // slot -> caller pair index
-  const double *itolsq;       // per slot beta^2
-  int32_t nslots;
+  const int32_t *slot_loops;   // 2 per slot
+  const double *itolsq;        // per slot beta^2
   double epssq;
-  double *lk;                 // per caller pair
-  double *err;                // per caller pair (Eq. 14 sum, unscaled)
-  double *counts;             // [0] far evals, [1] leaf evals
-  int2 *spill;                // kSpill per warp
-  int32_t tree_kind;          // 0 curve-order (root n/2 - 1), 1 kd (root n - 2)
-  unsigned long long *queue;  // [0] slot queue
-  int32_t *status;            // nonzero on overflow
+  const Batch *in;             // this round's batches
+  int64_t nin;
+  Batch *out;                  // batches left over for the next round
+  int64_t out_cap;
+  unsigned long long *out_count;
+  int32_t budget;              // iterations per batch before its stack is handed on
+  unsigned long long *acc_lk;  // per slot, fixed point (2^-40 turns)
+  unsigned long long *acc_err; // per slot, fixed point (2^-40)
+  double *counts;              // [0] far evals, [1] leaf evals
+  int2 *spill;                 // kSpill per warp
+  unsigned long long *queue;   // batch queue head
+  int32_t *status;             // nonzero on overflow
 };
+
+// Fixed-point (2^-40) accumulation: integer adds commute, so per-pair sums do
+// not depend on which warp finished first.
+constexpr double kFix = 1099511627776.0;  // 2^40
+__device__ __forceinline__ void fix_add(unsigned long long *a, double v) {
+  atomicAdd(a, (unsigned long long)__double2ll_rn(v * kFix));
+}
 
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
   return ax * bx + ay * by + az * bz;
@@ -425,6 +443,10 @@ __device__ void leaf_eval(const TravArgs &A, const NodeHdr &h1, const NodeHdr &h
   sum += kInvTwoPi * (double)atan2f(y, x) + (((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? (double)sg : 0.0);
 }
 
+// One warp per batch. The warp runs the two-tree traversal of its batch's
+// node pairs for at most `budget` steps; whatever is still on its stack then
+// is written out as new batches for the next round, so a heavy loop pair
+// spreads over many warps while light pairs finish in one go.
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
@@ -437,21 +459,20 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
   int2 *spill = A.spill + (size_t)gw * kSpill;
   double nfar = 0, nleaf = 0;
   for (;;) {
-    int slot = 0;
-    if (lane == 0) slot = (int)atomicAdd(A.queue, 1ULL);
-    slot = __shfl_sync(0xffffffffu, slot, 0);
-    if (slot >= A.nslots) break;
+    long long b = 0;
+    if (lane == 0) b = (long long)atomicAdd(A.queue, 1ULL);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (b >= A.nin) break;
+    const int slot = A.in[b].slot;
+    const int cnt0 = A.in[b].count;
     const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
     const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
     const NodeMom *M1 = A.mom + A.node_base[l1], *M2 = A.mom + A.node_base[l2];
     const double itolsq = A.itolsq[slot], eps = A.epssq;
-    int top = 0, nspill = 0, nf = 0, nl = 0;
+    if (lane < cnt0) stack[lane] = A.in[b].pairs[lane];
+    int top = cnt0, nspill = 0, nf = 0, nl = 0, steps = 0;
     bool overflow = false;
-    if (lane == 0)
-      stack[0] = A.tree_kind == 0 ? make_int2((int)(n1 / 2 - 1), (int)(n2 / 2 - 1))
-                                  : make_int2((int)(n1 - 2), (int)(n2 - 2));  // roots
-    top = 1;
     double sum = 0.0, err = 0.0;
     __syncwarp();
     while (true) {
@@ -463,6 +484,36 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
         __syncwarp();
       }
       if (top == 0) break;
+      if (steps >= A.budget) {  // hand the rest on as new batches
+        const int total = top + nspill;
+        const int nb = (total + 31) / 32;
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(A.out_count, (unsigned long long)nb);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if ((long long)(at + nb) <= A.out_cap) {
+          for (int q = 0; q < nb; ++q) {
+            const int e = 32 * q + lane;
+            if (e < total) A.out[at + q].pairs[lane] = e < nspill ? spill[e] : stack[e - nspill];
+            if (lane == 0) {
+              A.out[at + q].slot = slot;
+              A.out[at + q].count = min(32, total - 32 * q);
+            }
+          }
+          top = 0;
+          nspill = 0;
+          __syncwarp();
+          break;
+        }
+        // No room left: mark the reserved batches below the capacity empty
+        // and finish this batch here.
+        if (lane == 0)
+          for (int q = 0; q < nb && (long long)(at + q) < A.out_cap; ++q) {
+            A.out[at + q].slot = slot;
+            A.out[at + q].count = 0;
+          }
+        steps = INT_MIN;
+      }
+      ++steps;
       const int cnt = min(top, 32);
       const bool act = lane < cnt;
       int2 pr = make_int2(0, 0);
@@ -492,7 +543,6 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
           }
         }
       }
-      // push children
       const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
       const int ns = __popc(sm);
       if (top + 2 * ns > kStack) {  // spill the oldest half
@@ -515,7 +565,6 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
         stack[top + 2 * rank + 1] = c1;
       }
       top += 2 * ns;
-      // queue far and leaf pairs
       const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
       const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
       if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
@@ -523,46 +572,80 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
       nf += __popc(fm);
       nl += __popc(lm);
       __syncwarp();
-      const bool drain = (top == 0 && nspill == 0);
-      while (nf >= 32 || (drain && nf > 0)) {
-        const int k = min(nf, 32);
-        if (lane < k) {
-          const int2 q = farq[nf - k + lane];
-          const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
-          const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-          const double dsq = dx * dx + dy * dy + dz * dz + eps;
-          far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dsq, (float)h1.r, (float)h2.r, sum, err);
-        }
-        nfar += k;
-        nf -= k;
+      while (nf >= 32) {
+        const int2 q = farq[nf - 32 + lane];
+        const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+        far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
+                 (float)h1.r, (float)h2.r, sum, err);
+        nfar += 32;
+        nf -= 32;
         __syncwarp();
       }
-      while (nl >= 32 || (drain && nl > 0)) {
-        const int k = min(nl, 32);
-        if (lane < k) {
-          const int2 q = leafq[nl - k + lane];
-          leaf_eval(A, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
-        }
-        nleaf += k;
-        nl -= k;
+      while (nl >= 32) {
+        const int2 q = leafq[nl - 32 + lane];
+        leaf_eval(A, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+        nleaf += 32;
+        nl -= 32;
         __syncwarp();
       }
     }
+    // Evaluate what is still queued.
+    if (lane < nf) {
+      const int2 q = farq[lane];
+      const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+      const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+      far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
+               (float)h2.r, sum, err);
+    }
+    if (lane < nl) {
+      const int2 q = leafq[lane];
+      leaf_eval(A, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+    }
+    nfar += nf;
+    nleaf += nl;
+    __syncwarp();
     if (overflow && lane == 0) atomicExch(A.status, 1);
     for (int o = 16; o; o >>= 1) {
       sum += __shfl_xor_sync(0xffffffffu, sum, o);
       err += __shfl_xor_sync(0xffffffffu, err, o);
     }
     if (lane == 0) {
-      const int p = A.slot_pair[slot];
-      A.lk[p] = overflow ? __longlong_as_double(0x7ff8000000000000LL) : sum;
-      A.err[p] = err;
+      fix_add(A.acc_lk + slot, sum);
+      fix_add(A.acc_err + slot, err);
     }
   }
   if (lane == 0) {
     atomicAdd(A.counts, nfar);
     atomicAdd(A.counts + 1, nleaf);
   }
+}
+
+// Initial batches: the root pair of every slot in `slots`; clears their sums.
+__global__ void root_batches(const int32_t *slots, int64_t n, const int32_t *slot_loops, const int64_t *off,
+                             int32_t tree_kind, Batch *out, unsigned long long *acc_lk,
+                             unsigned long long *acc_err) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int s = slots[k];
+  const int l1 = slot_loops[2 * s], l2 = slot_loops[2 * s + 1];
+  const int64_t n1 = off[l1 + 1] - off[l1], n2 = off[l2 + 1] - off[l2];
+  out[k].slot = s;
+  out[k].count = 1;
+  out[k].pairs[0] = tree_kind == 0 ? make_int2((int)(n1 / 2 - 1), (int)(n2 / 2 - 1))
+                                   : make_int2((int)(n1 - 2), (int)(n2 - 2));
+  acc_lk[s] = 0;
+  acc_err[s] = 0;
+}
+
+// Fixed-point sums -> per caller pair doubles.
+__global__ void finish_sums(const unsigned long long *acc_lk, const unsigned long long *acc_err,
+                            const int32_t *slot_pair, int64_t nslots, double *lk, double *err) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  const int p = slot_pair[s];
+  lk[p] = (double)(long long)acc_lk[s] / kFix;
+  err[p] = (double)(long long)acc_err[s] / kFix;
 }
 
 __global__ void scatter_kernel(const double *src, const int32_t *idx, int64_t n, double *dst) {
@@ -721,8 +804,9 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaGetLastError());
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
   ++launches;
+  ctx.stats.ms_tree_build = ctx.elapsed(ctx.ev2, ctx.ev3);
 
-  // Traversal slots: order pairs by decreasing work.
+  // Slots: pairs ordered by decreasing estimated work.
   std::vector<int32_t> order(np);
   std::iota(order.begin(), order.end(), 0);
   std::vector<double> cost(np);
@@ -737,32 +821,66 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     slot_loops[2 * s] = h_pairs[2 * order[s]];
     slot_loops[2 * s + 1] = h_pairs[2 * order[s] + 1];
   }
-  int32_t *d_slots = ctx.d_bh[11].as<int32_t>(3 * np);
+  int32_t *d_slots = ctx.d_bh[11].as<int32_t>(4 * np);
   int32_t *d_slot_pair = d_slots + 2 * np;
+  int32_t *d_active = d_slots + 3 * np;
   double *d_itol = ctx.d_bh[12].as<double>(np);
   double *d_counts = ctx.d_bh[13].as<double>(2);
   int32_t *d_status = reinterpret_cast<int32_t *>(d_counts + 2);
-  unsigned long long *d_queue = ctx.d_counter.as<unsigned long long>(2);
+  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(2 * np + 4);
+  unsigned long long *d_acc_err = d_acc + np;
+  unsigned long long *d_ctr = d_acc + 2 * np;  // [0] queue, [1] next-round count
   int per_sm = 0;
   FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_traverse, 32 * kWarps, 0));
   per_sm = std::max(per_sm, 1);
-  const int64_t want = std::max<int64_t>(1, std::min<int64_t>((np + kWarps - 1) / kWarps, (int64_t)ctx.num_sms * per_sm));
-  const int grid = (int)want;
-  int2 *d_spill = ctx.d_bh[14].as<int2>((size_t)grid * kWarps * kSpill);
+  const int grid = ctx.num_sms * per_sm;
+  const int64_t nwarps = (int64_t)grid * kWarps;
+  int2 *d_spill = ctx.d_bh[14].as<int2>((size_t)nwarps * kSpill);
+  // Round buffers: a warp hands on at most (kStack + kSpill) / 32 + 1 batches.
+  const int64_t cap = std::max<int64_t>(np, nwarps * ((kStack + kSpill) / 32 + 1));
+  Batch *d_batch[2] = {reinterpret_cast<Batch *>(ctx.d_partial.need(2 * cap * sizeof(Batch))), nullptr};
+  d_batch[1] = d_batch[0] + cap;
   FLN_CUDA(cudaMemcpyAsync(d_slots, slot_loops.data(), 2 * np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_slot_pair, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-  const double b0 = prm.barnes_hut_init_beta;
-  std::vector<double> itol(np, b0 * b0);
-  FLN_CUDA(cudaMemcpyAsync(d_itol, itol.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
-  FLN_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), st));
-  ctx.stats.ms_tree_build = ctx.elapsed(ctx.ev2, ctx.ev3);
-  TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_slot_pair, d_itol, (int32_t)np, prm.epssq, d_lk_out,
-             d_err_out, d_counts, d_spill, prm.bh_tree == 1 ? 1 : 0, d_queue, d_status};
+  const double b0 = prm.barnes_hut_init_beta;
+  const int budget = 256;
+  ctx.stats.bh_rounds = 0;
+  // One Barnes–Hut pass over the slots in `active` with per-slot beta^2.
+  auto pass = [&](const std::vector<int32_t> &active, const std::vector<double> &itol_slots) {
+    const int64_t na = (int64_t)active.size();
+    FLN_CUDA(cudaMemcpyAsync(d_active, active.data(), na * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemcpyAsync(d_itol, itol_slots.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
+    root_batches<<<(int)((na + 255) / 256), 256, 0, st>>>(d_active, na, d_slots, d_off, prm.bh_tree == 1 ? 1 : 0,
+                                                          d_batch[0], d_acc, d_acc_err);
+    FLN_CUDA(cudaGetLastError());
+    ++launches;
+    int64_t nin = na;
+    int cur = 0;
+    for (int round = 0; nin > 0 && round < 4096; ++round) {
+      FLN_CUDA(cudaMemsetAsync(d_ctr, 0, 2 * sizeof(unsigned long long), st));
+      TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
+                 d_batch[1 - cur], cap, d_ctr + 1, budget, d_acc, d_acc_err, d_counts, d_spill, d_ctr, d_status};
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, grid));
+      bh_traverse<<<g, 32 * kWarps, 0, st>>>(A);
+      FLN_CUDA(cudaGetLastError());
+      ++launches;
+      ++ctx.stats.bh_rounds;
+      unsigned long long next = 0;
+      FLN_CUDA(cudaMemcpyAsync(&next, d_ctr + 1, sizeof next, cudaMemcpyDeviceToHost, st));
+      FLN_CUDA(cudaStreamSynchronize(st));
+      nin = (int64_t)std::min<unsigned long long>(next, (unsigned long long)cap);
+      cur = 1 - cur;
+    }
+  };
+  std::vector<int32_t> all(np);
+  std::iota(all.begin(), all.end(), 0);
+  std::vector<double> itol(np, b0 * b0);
   FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-  bh_traverse<<<grid, 32 * kWarps, 0, st>>>(A);
-  FLN_CUDA(cudaGetLastError());
+  pass(all, itol);
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+  finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
+  FLN_CUDA(cudaGetLastError());
   ++launches;
   // Error estimate and beta retry (lnc.cpp:165-184).
   std::vector<double> err(np);
@@ -771,45 +889,70 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
   FLN_CUDA(cudaStreamSynchronize(st));
   ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
-  std::vector<int32_t> flags(np, 0), rs_loops, rs_pair;
-  std::vector<double> rs_itol;
-  for (int64_t p = 0; p < np; ++p) {
+  std::vector<int32_t> flags(np, 0), retry_slots;
+  std::vector<char> retried(np, 0);
+  for (int64_t s = 0; s < np; ++s) {
+    const int64_t p = order[s];
     const double e = err[p] * prm.error_est_scale;
     err[p] = e;
     const double tb = std::min(std::pow(e / prm.target_error, 0.25) * b0, prm.barnes_hut_beta_limit);
     if (tb > b0) {
-      rs_loops.push_back(h_pairs[2 * p]);
-      rs_loops.push_back(h_pairs[2 * p + 1]);
-      rs_pair.push_back((int32_t)p);
-      rs_itol.push_back(tb * tb);
+      retry_slots.push_back((int32_t)s);
+      itol[s] = tb * tb;
       flags[p] |= FLN_PAIR_BETA_RETRIED;
+      retried[p] = 1;
     }
   }
+  ctx.stats.beta_retried = (int64_t)retry_slots.size();
   std::vector<double> far_leaf(2, 0.0);
-  if (!rs_pair.empty()) {
-    const int64_t nr = (int64_t)rs_pair.size();
-    FLN_CUDA(cudaMemcpyAsync(d_slots, rs_loops.data(), 2 * nr * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    FLN_CUDA(cudaMemcpyAsync(d_slot_pair, rs_pair.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    FLN_CUDA(cudaMemcpyAsync(d_itol, rs_itol.data(), nr * sizeof(double), cudaMemcpyHostToDevice, st));
-    FLN_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), st));
-    TravArgs R = A;
-    R.nslots = (int32_t)nr;
-    const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>((nr + kWarps - 1) / kWarps, grid));
+  if (!retry_slots.empty()) {
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-    bh_traverse<<<g2, 32 * kWarps, 0, st>>>(R);
-    FLN_CUDA(cudaGetLastError());
+    pass(retry_slots, itol);
     FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+    finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
+    FLN_CUDA(cudaGetLastError());
     ++launches;
-    // After a retry the reference keeps the new run's unscaled estimate.
+    // The reported estimate is that of the final run, scaled like the first
+    // (the reference stops using it after the retry; the margin check here
+    // needs both on one scale).
     std::vector<double> e2(np);
     FLN_CUDA(cudaMemcpyAsync(e2.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
     FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
     FLN_CUDA(cudaStreamSynchronize(st));
-    for (int32_t p : rs_pair) err[p] = e2[p];
-    ctx.stats.beta_retried = nr;
     ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
-  } else {
-    ctx.stats.beta_retried = 0;
+    for (int64_t p = 0; p < np; ++p)
+      if (retried[p]) err[p] = e2[p] * prm.error_est_scale;
+  }
+  // Escalation (beyond the reference): a pair whose estimate still exceeds
+  // bh_err_limit is re-run with twice its beta, up to bh_escalations times
+  // (beta <= 4 x beta_limit); what stays above goes to the FP64 direct sum.
+  ctx.stats.bh_escalated = 0;
+  for (int esc = 0; esc < prm.bh_escalations; ++esc) {
+    std::vector<int32_t> up;
+    for (int64_t s = 0; s < np; ++s) {
+      const int64_t p = order[s];
+      const double beta = std::sqrt(itol[s]);
+      if (!(err[p] <= prm.bh_err_limit) && beta < 4.0 * prm.barnes_hut_beta_limit) {
+        up.push_back((int32_t)s);
+        const double nb = std::min(2.0 * beta, 4.0 * prm.barnes_hut_beta_limit);
+        itol[s] = nb * nb;
+        flags[p] |= FLN_PAIR_BETA_ESCALATED;
+      }
+    }
+    if (up.empty()) break;
+    ctx.stats.bh_escalated += (int64_t)up.size();
+    FLN_CUDA(cudaEventRecord(ctx.ev2, st));
+    pass(up, itol);
+    FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+    finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
+    FLN_CUDA(cudaGetLastError());
+    ++launches;
+    std::vector<double> e3(np);
+    FLN_CUDA(cudaMemcpyAsync(e3.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+    ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+    for (int32_t s : up) err[order[s]] = e3[order[s]] * prm.error_est_scale;
   }
   FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   FLN_CUDA(cudaMemcpyAsync(d_err_out, err.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));

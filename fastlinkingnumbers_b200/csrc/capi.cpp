@@ -60,6 +60,7 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   ctx.stats.ms_tree_build = 0;
   ctx.stats.bh_far_evals = ctx.stats.bh_leaf_evals = 0;
   ctx.stats.beta_retried = 0;
+  ctx.stats.bh_escalated = 0;
   if (!d_err) d_err = ctx.d_err.as<double>(std::max<int64_t>(np, 1));  // Barnes–Hut needs one
   if (method == FLN_METHOD_DIRECTSUM) {
     launches += direct_sum_device(ctx, d_xyz, d_off, h_off, h_pairs, prm.precision, prm.near_factor, d_lk,
@@ -83,7 +84,7 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
       const double margin = 0.5 - std::fabs(lk[p] - r);
       // Low margin, non-finite, or a Barnes–Hut error estimate that could
       // reach the rounding boundary: recompute in FP64 direct sum.
-      if (!(margin >= prm.fp64_margin) || !(err[p] <= 0.5 - prm.fp64_margin)) {
+      if (!(margin >= prm.fp64_margin) || (method == FLN_METHOD_BARNESHUT && !(err[p] <= prm.bh_err_limit))) {
         redo_idx.push_back((int32_t)p);
         redo_pairs.push_back(h_pairs[2 * p]);
         redo_pairs.push_back(h_pairs[2 * p + 1]);
@@ -139,6 +140,7 @@ static fln_params resolved(const fln_params *p) {
     throw Error(FLN_ERR_INVALID_ARGUMENT, "unknown precision");
   if (!(r.barnes_hut_init_beta > 0) || !(r.barnes_hut_beta_limit > 0))
     throw Error(FLN_ERR_INVALID_ARGUMENT, "Barnes-Hut beta must be positive");
+  if (r.bh_escalations < 0 || r.bh_escalations > 8) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_escalations in [0, 8]");
   return r;
 }
 
@@ -245,6 +247,8 @@ void fln_default_params(fln_params *p) {
   p->fp64_margin = 0.25;
   p->near_factor = 1.0;
   p->bh_tree = 0;
+  p->bh_escalations = 2;
+  p->bh_err_limit = 0.25;
 }
 
 fln_status fln_ctx_create(int device, void *stream, fln_ctx **out) {

@@ -194,10 +194,45 @@ __global__ void __launch_bounds__(kBlockSegs) direct_fp64_kernel(DirectArgs A) {
 }
 
 // ------------------------------------------------------------------ mixed
+// arctan(t) for |t| <= 1/4 from its Maclaurin series t - t^3/3 + t^5/5 - t^7/7
+// + t^9/9; the first omitted term is below 2.2e-8 |t|, under FP32 rounding.
+__device__ __forceinline__ float atan_small(float t) {
+  const float u = t * t;
+  float p = fmaf(u, 1.0f / 9.0f, -1.0f / 7.0f);
+  p = fmaf(p, u, 1.0f / 5.0f);
+  p = fmaf(p, u, -1.0f / 3.0f);
+  p = fmaf(p, u, 1.0f);
+  return p * t;
+}
+
+// Minimum and maximum over the CTA of 7 values each (a box and a length);
+// the result is in out[0..6] (min) and out[7..13] (max) for every thread.
+__device__ __forceinline__ void block_minmax7(float *lo, float *hi, float (*s_box)[14], float *out) {
+  for (int o = 16; o; o >>= 1)
+    for (int v = 0; v < 7; ++v) {
+      lo[v] = fminf(lo[v], __shfl_xor_sync(0xffffffffu, lo[v], o));
+      hi[v] = fmaxf(hi[v], __shfl_xor_sync(0xffffffffu, hi[v], o));
+    }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int v = 0; v < 7; ++v) {
+      s_box[warp][v] = lo[v];
+      s_box[warp][7 + v] = hi[v];
+    }
+  __syncthreads();
+  for (int v = 0; v < 14; ++v) {
+    float r = s_box[0][v];
+    for (int w = 1; w < kBlockSegs / 32; ++w) r = v < 7 ? fminf(r, s_box[w][v]) : fmaxf(r, s_box[w][v]);
+    out[v] = r;
+  }
+}
+
 __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) {
   __shared__ float4 sq[kTile + 1];  // xyz relative to the tile origin; w = length of segment t
   __shared__ double s_red[kBlockSegs / 32];
+  __shared__ float s_box[kBlockSegs / 32][14];
   __shared__ long long s_item;
+  const float INF = __int_as_float(0x7f800000);
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) s_item = (long long)atomicAdd(A.counter, 1ULL);
@@ -231,49 +266,83 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
         sq[t] = make_float4((float)(v.x - O.x), (float)(v.y - O.y), (float)(v.z - O.z), 0.f);
       }
       __syncthreads();
+      const float r0x = (float)(p0.x - O.x), r0y = (float)(p0.y - O.y), r0z = (float)(p0.z - O.z);
+      const float r1x = (float)(p1.x - O.x), r1y = (float)(p1.y - O.y), r1z = (float)(p1.z - O.z);
+      // Boxes of this thread's curve-1 segment (slots 0-2, length 3) and of
+      // its curve-2 tile vertices (slots 4-6, length 3 of the max).
+      float lo[7], hi[7];
+      for (int v = 0; v < 7; ++v) {
+        lo[v] = INF;
+        hi[v] = -INF;
+      }
+      if (active) {
+        lo[0] = fminf(r0x, r1x); hi[0] = fmaxf(r0x, r1x);
+        lo[1] = fminf(r0y, r1y); hi[1] = fmaxf(r0y, r1y);
+        lo[2] = fminf(r0z, r1z); hi[2] = fmaxf(r0z, r1z);
+        hi[3] = len1;
+      }
       for (int t = threadIdx.x; t < kt; t += kBlockSegs) {
         const float4 a = sq[t], b = sq[t + 1];
         const float fx = b.x - a.x, fy = b.y - a.y, fz = b.z - a.z;
-        sq[t].w = sqrtf(fx * fx + fy * fy + fz * fz);
+        const float len = sqrtf(fx * fx + fy * fy + fz * fz);
+        sq[t].w = len;
+        lo[4] = fminf(lo[4], fminf(a.x, b.x)); hi[4] = fmaxf(hi[4], fmaxf(a.x, b.x));
+        lo[5] = fminf(lo[5], fminf(a.y, b.y)); hi[5] = fmaxf(hi[5], fmaxf(a.y, b.y));
+        lo[6] = fminf(lo[6], fminf(a.z, b.z)); hi[6] = fmaxf(hi[6], fmaxf(a.z, b.z));
+        hi[3] = fmaxf(hi[3], len);
       }
+      float bx[14];
+      block_minmax7(lo, hi, s_box, bx);
       __syncthreads();
+      // Box gap between the CTA's curve-1 segments and this tile: no segment
+      // pair can be near-singular when it exceeds near_factor x (longest segment).
+      const float gx = fmaxf(0.f, fmaxf(bx[4] - bx[7], bx[0] - bx[11]));
+      const float gy = fmaxf(0.f, fmaxf(bx[5] - bx[8], bx[1] - bx[12]));
+      const float gz = fmaxf(0.f, fmaxf(bx[6] - bx[9], bx[2] - bx[13]));
+      const float lim = A.near_factor * bx[10];
+      const bool far_tile = gx * gx + gy * gy + gz * gz > 1.0001f * lim * lim;
       if (!active) continue;
-      const float r0x = (float)(p0.x - O.x), r0y = (float)(p0.y - O.y), r0z = (float)(p0.z - O.z);
-      const float r1x = (float)(p1.x - O.x), r1y = (float)(p1.y - O.y), r1z = (float)(p1.z - O.z);
       float4 q = sq[0];
       float ax = q.x - r0x, ay = q.y - r0y, az = q.z - r0z;
-      float bx = q.x - r1x, by = q.y - r1y, bz = q.z - r1z;
-      float la = sqrtf(ax * ax + ay * ay + az * az), lb = sqrtf(bx * bx + by * by + bz * bz);
-      float ab = ax * bx + ay * by + az * bz;
+      float bx_ = q.x - r1x, by = q.y - r1y, bz = q.z - r1z;
+      float la = sqrtf(ax * ax + ay * ay + az * az), lb = sqrtf(bx_ * bx_ + by * by + bz * bz);
+      float ab = ax * bx_ + ay * by + az * bz;
       float accf = 0.f;
       for (int k = 0; k < kt; ++k) {
         const float4 qn = sq[k + 1];
         const float cx = qn.x - r1x, cy = qn.y - r1y, cz = qn.z - r1z;
         const float dx = qn.x - r0x, dy = qn.y - r0y, dz = qn.z - r0z;
-        const float lc = sqrtf(cx * cx + cy * cy + cz * cz), ld = sqrtf(dx * dx + dy * dy + dz * dz);
+        const float cc = cx * cx + cy * cy + cz * cz, dd = dx * dx + dy * dy + dz * dz;
+        const float lc = cc * rsqrtf(cc), ld = dd * rsqrtf(dd);
         const float cd = cx * dx + cy * dy + cz * dz;
-        const float close = fminf(fminf(la, lb), fminf(lc, ld));
-        if (close < A.near_factor * fmaxf(len1, q.w)) {
+        bool near = false;
+        if (!far_tile) near = fminf(fminf(la, lb), fminf(lc, ld)) < A.near_factor * fmaxf(len1, q.w);
+        if (near) {
           const int64_t kk = k0 + k, kn = kk + 1;
           near_turns += term_fp64(p0, p1, load_v(A.xyz, o2 + kk), load_v(A.xyz, o2 + (kn == n2 ? 0 : kn)));
           ++near_count;
         } else {
           const float ca = cx * ax + cy * ay + cz * az;
-          const float cb = cx * bx + cy * by + cz * bz;
+          const float cb = cx * bx_ + cy * by + cz * bz;
           const float ad = ax * dx + ay * dy + az * dz;
           const float fx = qn.x - q.x, fy = qn.y - q.y, fz = qn.z - q.z;
           const float det = ax * (fy * ez - fz * ey) + ay * (fz * ex - fx * ez) + az * (fx * ey - fy * ex);
           const float t = la * lc;
           const float div1 = t * lb + ab * lc + ca * lb + cb * la;
           const float div2 = t * ld + ad * lc + ca * ld + cd * la;
+          const float sdiv = div1 + div2;
           const float xp = div1 * div2 - det * det;
-          const float yp = det * (div1 + div2);
-          accf += atan2f(yp, xp);
-          if (yp * det < 0.f) turns += (det > 0.f) ? 1 : -1;
+          const float yp = det * sdiv;
+          if (sdiv > 0.f && fabsf(yp) < 0.25f * xp) {
+            accf += atan_small(__fdividef(yp, xp));  // principal branch, |angle| < 0.245
+          } else {
+            accf += atan2f(yp, xp);
+            if (sdiv < 0.f && det != 0.f) turns += (det > 0.f) ? 1 : -1;
+          }
         }
         q = qn;
         ax = dx; ay = dy; az = dz;
-        bx = cx; by = cy; bz = cz;
+        bx_ = cx; by = cy; bz = cz;
         la = ld; lb = lc; ab = cd;
       }
       acc += (double)accf;

@@ -63,7 +63,8 @@ enum {
   FLN_PAIR_FP64_RECOMPUTED = 1, /* margin below threshold or non-finite: recomputed in FP64 direct sum */
   FLN_PAIR_BETA_RETRIED = 2,    /* Barnes–Hut re-run with the larger beta (lnc.cpp:165-184) */
   FLN_PAIR_NONFINITE = 4,       /* still non-finite after the recompute */
-  FLN_PAIR_SWAPPED = 8          /* evaluated with the loops' roles exchanged (symmetric) */
+  FLN_PAIR_SWAPPED = 8,         /* evaluated with the loops' roles exchanged (symmetric) */
+  FLN_PAIR_BETA_ESCALATED = 16  /* Barnes–Hut re-run with a beta beyond the reference's rule */
 };
 
 typedef struct fln_params {
@@ -78,7 +79,11 @@ typedef struct fln_params {
                                    below near_factor * (longer segment length) is evaluated in FP64; 1.0 */
   int32_t bh_tree;              /* Barnes–Hut tree: 0 = curve-order tree (default), 1 = the reference's
                                    kd-median tree (ModifiedKdBVH.h:207-237) */
-  int32_t reserved[7];
+  int32_t bh_escalations;       /* after the reference's retry, a pair whose scaled error estimate is still
+                                   above bh_err_limit is re-run with twice its beta, up to this many times;
+                                   default 2 (0 = the reference's behaviour) */
+  double bh_err_limit;          /* default 0.25; a pair still above it is recomputed by FP64 direct sum */
+  int32_t reserved[4];
 } fln_params;
 
 /* Statistics of the last computation on a context. */
@@ -99,6 +104,9 @@ typedef struct fln_stats {
   double ms_main_kernel;        /* device time of the dominant kernel(s): the Barnes–Hut traversal or the
                                    direct-sum kernel (CUDA events on the launching stream) */
   double ms_tree_build;         /* Barnes–Hut tree topology + FP64 moment build */
+  int32_t bh_rounds;            /* Barnes–Hut traversal launches (work is handed on between rounds) */
+  int32_t reserved_stats;
+  int64_t bh_escalated;         /* pair re-runs with an escalated beta */
 } fln_stats;
 
 typedef struct fln_ctx fln_ctx;

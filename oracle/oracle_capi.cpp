@@ -142,13 +142,14 @@ int orc_eval_pairs(void *m, int method, const int32_t *pi, const int32_t *pj, in
     auto *o = static_cast<OrcModel *>(m);
     const int nc = (int)o->poly.size();
     if (nthreads > 0) omp_set_num_threads(nthreads);
-    if (method == 2 && (int)o->trees.size() != nc) {
-      o->trees.assign(nc, SegTree());
+    if (method == 2) {
+      // Trees are built once per loop, on first use.
+      if ((int)o->trees.size() != nc) o->trees.assign(nc, SegTree());
       std::vector<char> need(nc, 0);
       for (int64_t p = 0; p < n; ++p) need[pi[p]] = need[pj[p]] = 1;
 #pragma omp parallel for schedule(dynamic)
       for (int i = 0; i < nc; ++i)
-        if (need[i]) o->trees[i] = make_seg_tree(o->poly[i]);
+        if (need[i] && o->trees[i].mom.empty()) o->trees[i] = make_seg_tree(o->poly[i]);
     }
     std::string err;
 #pragma omp parallel for schedule(dynamic) if (!(method == 2 && bh_parallel) && !(method == 1))
@@ -171,6 +172,7 @@ int orc_eval_pairs(void *m, int method, const int32_t *pi, const int32_t *pj, in
             uint64_t nf2 = 0, nl2 = 0;
             e = 0;
             lk = bh_eval(t1, t2, 1e-24, tb * tb, e, bh_parallel, &nf2, &nl2);
+            e *= 0.05;  // reported on the first run's scale
             nf += nf2;
             nl += nl2;
           }

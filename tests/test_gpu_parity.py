@@ -75,7 +75,8 @@ def test_barneshut_reference_tree_matches_oracle(engine, name, golden_dir):
     _, off, xyz, pairs = _prepared(name, golden_dir)
     o = pyoracle.Oracle().set_polylines(off, xyz)
     lk_o, err_o, _, _ = o.eval_pairs(pyoracle.BARNES_HUT, pairs, bh_parallel=True)
-    lk, err, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_tree=1, fp64_margin=0.0)
+    lk, err, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_tree=1, fp64_margin=0.0,
+                                        bh_escalations=0, bh_err_limit=1e30)
     np.testing.assert_allclose(lk, lk_o, rtol=0, atol=2e-5)
     np.testing.assert_allclose(err, err_o, rtol=1e-3, atol=1e-9)
 
@@ -141,10 +142,10 @@ def test_chain_mail_full_size(engine):
 
 
 def test_beta_retry_path(engine, golden_dir):
-    # A tiny initial beta forces the reference's retry rule (lnc.cpp:165-184).
+    # A small initial beta forces the reference's retry rule (lnc.cpp:165-184).
     _, off, xyz, pairs = _prepared("knittubebroken", golden_dir)
     ref = np.load(os.path.join(GOLDEN, "pairs", "knittubebroken.npz"))
-    lk, err, flags = engine.linking_numbers(xyz, off, pairs, "barneshut", barnes_hut_init_beta=0.5)
+    lk, err, flags = engine.linking_numbers(xyz, off, pairs, "barneshut", barnes_hut_init_beta=1.0)
     assert (flags & N.PAIR_BETA_RETRIED).any()
     assert np.array_equal(np.round(lk), np.round(ref["lk_direct"]))
 
@@ -156,6 +157,11 @@ def test_low_margin_pairs_are_recomputed_in_fp64(engine, golden_dir):
     ref = np.load(os.path.join(GOLDEN, "pairs", "knittubeinit.npz"))
     lk, _, flags = engine.linking_numbers(xyz, off, pairs, "barneshut", fp64_margin=0.5)
     assert (flags & N.PAIR_FP64_RECOMPUTED).all()
+    lk2, err2, flags2 = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_err_limit=0.0,
+                                               bh_escalations=1)
+    # Every pair is escalated once (beta x2) and then recomputed in FP64.
+    assert (flags2 & N.PAIR_BETA_ESCALATED).all() and (flags2 & N.PAIR_FP64_RECOMPUTED).all()
+    np.testing.assert_allclose(lk2, ref["lk_direct"], rtol=0, atol=1e-9)
     np.testing.assert_allclose(lk, ref["lk_direct"], rtol=0, atol=1e-9)
 
 
