@@ -32,7 +32,7 @@ PAIR_BETA_ESCALATED = 16
 EXPORTED = [
     "fln_status_string", "fln_last_error", "fln_abi_version", "fln_default_params",
     "fln_ctx_create", "fln_ctx_destroy", "fln_ctx_stats", "fln_linking_numbers",
-    "fln_linking_numbers_device", "fln_direct_pair", "fln_model_create", "fln_model_destroy",
+    "fln_linking_numbers_device", "fln_linking_numbers_direct_noalloc", "fln_direct_pair", "fln_model_create", "fln_model_destroy",
     "fln_model_load_bcc", "fln_model_save_bcc", "fln_model_set_curves", "fln_model_num_curves",
     "fln_model_num_points", "fln_model_get_curves", "fln_model_prepare",
     "fln_model_prepared_sizes", "fln_model_get_prepared", "fln_certificate_compute",
@@ -103,6 +103,7 @@ def load():
     L.fln_linking_numbers_device.argtypes = [vp, vp, vp, i32, vp, i64, C.c_int, P(Params), vp, vp,
                                              vp]
     L.fln_direct_pair.argtypes = [vp, vp, i64, vp, i64, i32, P(f64)]
+    L.fln_linking_numbers_direct_noalloc.argtypes = [vp, vp, i32, vp, i64, i32, vp, vp]
     L.fln_model_create.argtypes = [P(vp)]
     L.fln_model_destroy.argtypes = [vp]
     L.fln_model_load_bcc.argtypes = [vp, C.c_char_p]

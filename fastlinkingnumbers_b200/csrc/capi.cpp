@@ -159,6 +159,10 @@ struct fln_certificate {
   Certificate c;
 };
 
+namespace fln {
+void set_last_error(const std::string &msg);
+}
+
 namespace {
 thread_local std::string g_last_error;
 
@@ -210,6 +214,8 @@ void compute_pairs_host(Context &ctx, const double *xyz, const int64_t *loop_off
   ctx.stats.ms_total = now_ms() - t0;
 }
 }  // namespace
+
+void fln::set_last_error(const std::string &msg) { g_last_error = msg; }
 
 extern "C" {
 

@@ -38,7 +38,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
+#include <string>
 
 #include "engine.hpp"
 
@@ -428,3 +430,213 @@ int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
 }
 
 }  // namespace fln
+
+// ---------------------------------------------------------------------------
+// Direct sum that allocates nothing (fln_linking_numbers_direct_noalloc).
+//
+// Some callers cannot call cudaMalloc: code that runs while another framework
+// owns the device's memory pool (a renderer or simulator with its own
+// allocator and a fixed budget), code that must not add allocator
+// synchronisation or fragmentation to a latency-critical loop, and code on
+// paths where an allocation failure cannot be handled. For them the direct
+// sum runs entirely in the caller's input and output buffers plus one
+// file-scope device array, g_noalloc_scratch, of kNoAllocScratchBytes
+// (about 9.3 MB). Every GPU that loads libfln.so holds that array until the
+// process exits. Limits: at most kNoAllocMaxPairs loop pairs per call and
+// kNoAllocMaxItems work items (one item = 128 segments of the longer loop of
+// a pair, summed over the pairs); larger calls are rejected with
+// FLN_ERR_INVALID_ARGUMENT before any kernel runs on them.
+//
+// In host code the name g_noalloc_scratch only stands for the array: its
+// device address is obtained once per device with cudaGetSymbolAddress, on
+// the first call made with that device current, and cached. That first call
+// therefore does the set-up and should come before any stream capture.
+// All calls share the array and it keeps the previous call's contents: the
+// planning kernel clears the work-queue counters at the start of every call.
+// Calls whose work overlaps on the GPU (different streams, or host threads
+// racing) race on the array; issue them one after another.
+namespace fln {
+namespace {
+
+constexpr int64_t kNoAllocMaxPairs = 65536;
+constexpr int64_t kNoAllocMaxItems = int64_t(1) << 20;
+constexpr size_t kNaHeader = 256;  // counters[2], total items, status
+constexpr size_t kNaLoops = kNaHeader;                                       // int32 x 2 per pair
+constexpr size_t kNaOrder = kNaLoops + 2 * kNoAllocMaxPairs * 4;             // int32 per pair
+constexpr size_t kNaStart = kNaOrder + kNoAllocMaxPairs * 4;                 // int64 per pair + 1
+constexpr size_t kNaPartial = (kNaStart + (kNoAllocMaxPairs + 1) * 8 + 255) / 256 * 256;  // double per item
+constexpr size_t kNoAllocScratchBytes = kNaPartial + kNoAllocMaxItems * 8;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NaHeader {
+  unsigned long long counter[2];  // work queue head, near-singular term count
+  long long total_items;
+  int status;                     // bit 0: bad pair index, bit 1: loop with < 2 vertices
+};
+
+// One CTA plans the call inside the scratch array: orients each pair (longer
+// loop first), counts its items, scans them into item_start and clears the
+// counters the direct-sum kernels start from.
+__global__ void __launch_bounds__(1024) noalloc_plan(const int64_t *off, int32_t nloops, const int32_t *pairs,
+                                                     int64_t npairs, unsigned char *scratch) {
+  NaHeader *h = reinterpret_cast<NaHeader *>(scratch);
+  int32_t *loops = reinterpret_cast<int32_t *>(scratch + kNaLoops);
+  int32_t *order = reinterpret_cast<int32_t *>(scratch + kNaOrder);
+  int64_t *start = reinterpret_cast<int64_t *>(scratch + kNaStart);
+  __shared__ long long s_warp[32];
+  __shared__ long long s_carry;
+  __shared__ int s_status;
+  if (threadIdx.x == 0) {
+    s_carry = 0;
+    s_status = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t base = 0; base < npairs; base += 1024) {
+    const int64_t p = base + threadIdx.x;
+    long long items = 0;
+    if (p < npairs) {
+      int a = pairs[2 * p], b = pairs[2 * p + 1];
+      if (a < 0 || a >= nloops || b < 0 || b >= nloops || a == b) {
+        atomicOr(&s_status, 1);
+      } else {
+        int64_t na = off[a + 1] - off[a], nb = off[b + 1] - off[b];
+        if (na < 2 || nb < 2) {
+          atomicOr(&s_status, 2);
+        } else {
+          if (nb > na) {
+            const int t = a;
+            a = b;
+            b = t;
+            const int64_t tn = na;
+            na = nb;
+            nb = tn;
+          }
+          items = (na + kBlockSegs - 1) / kBlockSegs;
+        }
+      }
+      loops[2 * p] = a;
+      loops[2 * p + 1] = b;
+      order[p] = (int32_t)p;
+    }
+    // Exclusive block scan of `items`.
+    long long incl = items;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      long long v = s_warp[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+      }
+      s_warp[lane] = v;  // inclusive over warps
+    }
+    __syncthreads();
+    const long long warp_base = warp ? s_warp[warp - 1] : 0;
+    if (p < npairs) start[p] = s_carry + warp_base + incl - items;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += s_warp[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    start[npairs] = s_carry;
+    h->counter[0] = 0;
+    h->counter[1] = 0;
+    h->total_items = s_carry;
+    h->status = s_status;
+  }
+}
+
+// Device address of g_noalloc_scratch per device, set up on first use.
+void *noalloc_scratch_for_current_device(fln_status &st, std::string &msg) {
+  static void *addr[64] = {nullptr};
+  static std::mutex mu;
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    st = e == cudaSuccess ? FLN_ERR_INVALID_ARGUMENT : FLN_ERR_NO_DEVICE;
+    msg = std::string("cudaGetDevice: ") + (e == cudaSuccess ? "device index >= 64" : cudaGetErrorString(e));
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      st = FLN_ERR_CUDA;
+      msg = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
+      return nullptr;
+    }
+    addr[dev] = p;
+  }
+  return addr[dev];
+}
+
+}  // namespace
+
+// Records the message behind a non-OK status for fln_last_error() (capi.cpp).
+void set_last_error(const std::string &msg);
+
+}  // namespace fln
+
+extern "C" fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, const int64_t *d_loop_offsets,
+                                                         int32_t nloops, const int32_t *d_pairs, int64_t npairs,
+                                                         int32_t precision, double *d_lk_out, void *stream) {
+  using namespace fln;
+  auto fail = [](fln_status s, const std::string &m) {
+    set_last_error(m);
+    return s;
+  };
+  if (npairs < 0 || npairs > kNoAllocMaxPairs)
+    return fail(FLN_ERR_INVALID_ARGUMENT, "fln_linking_numbers_direct_noalloc: npairs must be in [0, " +
+                                              std::to_string(kNoAllocMaxPairs) + "], got " + std::to_string(npairs));
+  if (nloops < 0 || (npairs > 0 && (!d_xyz || !d_loop_offsets || !d_pairs || !d_lk_out)))
+    return fail(FLN_ERR_INVALID_ARGUMENT, "fln_linking_numbers_direct_noalloc: NULL or negative argument");
+  if (precision != FLN_PREC_FP64 && precision != FLN_PREC_MIXED)
+    return fail(FLN_ERR_INVALID_ARGUMENT, "fln_linking_numbers_direct_noalloc: unknown precision");
+  if (npairs == 0) return FLN_OK;
+  fln_status st = FLN_OK;
+  std::string msg;
+  unsigned char *scratch = static_cast<unsigned char *>(noalloc_scratch_for_current_device(st, msg));
+  if (!scratch) return fail(st, msg);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  noalloc_plan<<<1, 1024, 0, s>>>(d_loop_offsets, nloops, d_pairs, npairs, scratch);
+  NaHeader h;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, scratch, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(FLN_ERR_CUDA, std::string("fln_linking_numbers_direct_noalloc: ") + cudaGetErrorString(e));
+  if (h.status & 1) return fail(FLN_ERR_INVALID_ARGUMENT, "fln_linking_numbers_direct_noalloc: pair index out of range or a pair names one loop twice");
+  if (h.status & 2) return fail(FLN_ERR_INVALID_ARGUMENT, "fln_linking_numbers_direct_noalloc: every loop in a pair needs at least two vertices");
+  if (h.total_items > kNoAllocMaxItems)
+    return fail(FLN_ERR_INVALID_ARGUMENT, "fln_linking_numbers_direct_noalloc: " + std::to_string(h.total_items) +
+                                              " work items exceed the limit of " + std::to_string(kNoAllocMaxItems) +
+                                              " (one item = 128 segments of the longer loop of a pair)");
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  DirectArgs A{d_xyz, d_loop_offsets, reinterpret_cast<const int32_t *>(scratch + kNaLoops),
+               reinterpret_cast<const int64_t *>(scratch + kNaStart), (int32_t)npairs, h.total_items,
+               reinterpret_cast<double *>(scratch + kNaPartial), reinterpret_cast<unsigned long long *>(scratch),
+               1.0f};
+  if (precision == FLN_PREC_FP64) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel, kBlockSegs, 0);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));
+    direct_fp64_kernel<<<grid, kBlockSegs, 0, s>>>(A);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel, kBlockSegs, 0);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));
+    direct_mixed_kernel<<<grid, kBlockSegs, 0, s>>>(A);
+  }
+  reduce_items_kernel<<<(int)((npairs + 255) / 256), 256, 0, s>>>(
+      reinterpret_cast<const double *>(scratch + kNaPartial), reinterpret_cast<const int64_t *>(scratch + kNaStart),
+      reinterpret_cast<const int32_t *>(scratch + kNaOrder), (int32_t)npairs, d_lk_out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(FLN_ERR_CUDA, std::string("fln_linking_numbers_direct_noalloc: ") + cudaGetErrorString(e));
+  return FLN_OK;
+}

@@ -149,6 +149,26 @@ fln_status fln_linking_numbers_device(fln_ctx *ctx, const double *d_xyz,
                                       const fln_params *params, double *d_lk_out,
                                       double *d_err_out, int32_t *d_flags_out);
 
+/* Direct sum that allocates no memory. No counterpart in the reference.
+ * For callers that cannot call cudaMalloc — code running while another
+ * framework owns the device's memory pool, latency-critical loops that must
+ * not take allocator locks, or paths where an allocation failure cannot be
+ * handled. Every array is the caller's device memory; the only other memory
+ * used is one fixed device array inside libfln.so (about 9.3 MB per GPU,
+ * held until the process exits). Limits: npairs <= 65536 and at most 2^20
+ * work items (one item = 128 segments of the longer loop of a pair, summed
+ * over pairs); larger calls return FLN_ERR_INVALID_ARGUMENT. precision is
+ * FLN_PREC_FP64 or FLN_PREC_MIXED; the results are the raw sums of that
+ * precision (no margin recompute). Work is queued on `stream` (a
+ * cudaStream_t, NULL = default stream) of the current device; the call
+ * waits for a small planning step and returns with the sums still in flight
+ * on `stream`. The first call on a device looks up the array's device
+ * address, so make it before any stream capture. Calls share the array:
+ * calls whose work overlaps on the GPU race, so issue them one at a time. */
+fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, const int64_t *d_loop_offsets,
+                                              int32_t nloops, const int32_t *d_pairs, int64_t npairs,
+                                              int32_t precision, double *d_lk_out, void *stream);
+
 /* One pair, host arrays (compute_link.h:62-64 and :86-87). */
 fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const double *xyz2,
                            int64_t n2, int32_t precision, double *lk_out);
