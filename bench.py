@@ -65,6 +65,8 @@ def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000):
         cfg = {"workload": "ring chain: 64 rings x 32 segments", "loops": 64}
     else:
         raise SystemExit(f"unknown workload {name}")
+    cfg.update({"method": "barneshut (quadrupole, beta 2, beta_limit 10)", "seed": seed,
+                "l2": "inputs and per-step trees larger than L2 (no flush needed)"})
     m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
     t0 = time.perf_counter()
     poff, pxyz, pairs, rounds = m.Prepare(True)
@@ -161,7 +163,10 @@ def run_reference(args, rank):
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * info["seconds"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": cfg,
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": dict(cfg, parallelism=f"replicas x{args.gpus}"),
+        "impl_details": {"method": "barneshut", "precision": "f64",
+                         "tree": "reference kd-median", "traversal": "serial depth-first per pair"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -266,10 +271,9 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": dict(cfg, method=args.method, precision=args.precision,
-                       tree="curve-order" if args.bh_tree == 0 else "reference kd-median",
-                       l2="inputs and per-step trees larger than L2 (no flush needed)",
-                       parallelism=f"replicas x{world}"),
+        "config": dict(cfg, parallelism=f"replicas x{world}"),
+        "impl_details": {"method": args.method, "precision": args.precision,
+                         "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median"},
         "certificate_ms": ms,
         "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(pxyz.nbytes + poff.nbytes + pairs.nbytes),
