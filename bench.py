@@ -186,7 +186,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     eng = Engine(local_rank, stream.cuda_stream)
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
-                           bh_tree=args.bh_tree)
+                           bh_tree=args.bh_tree, bh_schedule=args.bh_schedule)
     d_xyz = torch.from_numpy(pxyz).cuda()
     d_off = torch.from_numpy(poff).cuda()
     d_pairs = torch.from_numpy(pairs).cuda()
@@ -208,7 +208,8 @@ def run_ours(args, rank, world, local_rank):
         s = step()
         print(f"[bench] warmup {w}: {1e3 * (time.perf_counter() - t0):.1f} ms wall, main kernel "
               f"{s['ms_main_kernel']:.1f} ms, tree {s['ms_tree_build']:.1f} ms, far {s['bh_far_evals']:.3g}, "
-              f"leaf {s['bh_leaf_evals']:.3g}, retried {s['beta_retried']}, fp64 {s['fp64_recomputed']}",
+              f"leaf {s['bh_leaf_evals']:.3g}, retried {s['beta_retried']}, escalated {s['bh_escalated']}, "
+              f"fp64 {s['fp64_recomputed']}, launches {s['kernel_launches']}, timeouts {s['bh_wait_timeouts']}",
               file=sys.stderr, flush=True)
     torch.cuda.synchronize()
     if world > 1:
@@ -273,7 +274,8 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
         "config": dict(cfg, parallelism=f"replicas x{world}"),
         "impl_details": {"method": args.method, "precision": args.precision,
-                         "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median"},
+                         "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median",
+                         "schedule": "budgeted rounds" if args.bh_schedule == 0 else "persistent queue"},
         "certificate_ms": ms,
         "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(pxyz.nbytes + poff.nbytes + pairs.nbytes),
@@ -282,6 +284,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof,
         "clocks": clk,
         "stats": {"pairs": npairs, "segment_pairs": units, "beta_retried": s_last["beta_retried"],
+                  "escalated": s_last["bh_escalated"], "wait_timeouts": s_last["bh_wait_timeouts"],
                   "fp64_recomputed": s_last["fp64_recomputed"], "tree_build_ms": s_last["ms_tree_build"],
                   "far_evals": s_last["bh_far_evals"], "leaf_evals": s_last["bh_leaf_evals"],
                   "nonzero_links": int(np.sum(np.round(lk) != 0)), "flags_recomputed": int(np.sum(flags & 1))},
@@ -326,6 +329,7 @@ def main():
     ap.add_argument("--method", default="barneshut", choices=["barneshut", "directsum"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--bh-tree", type=int, default=0)
+    ap.add_argument("--bh-schedule", type=int, default=0, help="0 budgeted rounds, 1 persistent queue")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--loops", type=int, default=200)
     ap.add_argument("--loop-steps", type=int, default=50000)

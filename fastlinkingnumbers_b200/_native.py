@@ -49,7 +49,7 @@ class Params(C.Structure):
         ("epssq", C.c_double), ("target_error", C.c_double), ("error_est_scale", C.c_double),
         ("precision", C.c_int32), ("fp64_margin", C.c_double), ("near_factor", C.c_double),
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
-        ("reserved", C.c_int32 * 4),
+        ("bh_schedule", C.c_int32), ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -62,7 +62,7 @@ class Stats(C.Structure):
         ("max_off_integer", C.c_double), ("discretize_rounds", C.c_int32),
         ("kernel_launches", C.c_int32), ("ms_main_kernel", C.c_double),
         ("ms_tree_build", C.c_double), ("bh_rounds", C.c_int32), ("reserved_stats", C.c_int32),
-        ("bh_escalated", C.c_int64),
+        ("bh_escalated", C.c_int64), ("bh_wait_timeouts", C.c_int64),
     ]
 
     def as_dict(self):

@@ -416,7 +416,7 @@ __device__ __noinline__ double seg_term_fp64(const double *xyz, int64_t p0i, int
 // Exact leaf-leaf term in FP32 from the separation and the two tangents
 // (compute_link.cpp:576-606); FP64 from the vertices when the segments are
 // closer than their length.
-__device__ void leaf_eval(const TravArgs &A, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &m1,
+__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &m1,
                           const NodeMom &m2, int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
   const float rx = (float)(h2.m[0] - h1.m[0]), ry = (float)(h2.m[1] - h1.m[1]), rz = (float)(h2.m[2] - h1.m[2]);
   const float t1x = m1.t[0], t1y = m1.t[1], t1z = m1.t[2];
@@ -429,7 +429,7 @@ __device__ void leaf_eval(const TravArgs &A, const NodeHdr &h1, const NodeHdr &h
   const float lc = sqrtf(dot3(gax, gay, gaz, gax, gay, gaz)), ld = sqrtf(dot3(dex, dey, dez, dex, dey, dez));
   if (fminf(fminf(la, lb), fminf(lc, ld)) < fmaxf(m1.tn, m2.tn)) {
     const int64_t s1 = -1 - h1.left, s2 = -1 - h2.left;
-    sum += seg_term_fp64(A.xyz, o1 + s1, o1 + (s1 + 1 == n1 ? 0 : s1 + 1), o2 + s2, o2 + (s2 + 1 == n2 ? 0 : s2 + 1));
+    sum += seg_term_fp64(xyz, o1 + s1, o1 + (s1 + 1 == n1 ? 0 : s1 + 1), o2 + s2, o2 + (s2 + 1 == n2 ? 0 : s2 + 1));
     return;
   }
   const float det = rx * (t2y * t1z - t2z * t1y) + ry * (t2z * t1x - t2x * t1z) + rz * (t2x * t1y - t2y * t1x);
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
       }
       while (nl >= 32) {
         const int2 q = leafq[nl - 32 + lane];
-        leaf_eval(A, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+        leaf_eval(A.xyz, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
         nleaf += 32;
         nl -= 32;
         __syncwarp();
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
     }
     if (lane < nl) {
       const int2 q = leafq[lane];
-      leaf_eval(A, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+      leaf_eval(A.xyz, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
     }
     nfar += nf;
     nleaf += nl;
@@ -646,6 +646,381 @@ __global__ void finish_sums(const unsigned long long *acc_lk, const unsigned lon
   const int p = slot_pair[s];
   lk[p] = (double)(long long)acc_lk[s] / kFix;
   err[p] = (double)(long long)acc_err[s] / kFix;
+}
+
+// ------------------------------------------------------------------ persistent traversal
+// One launch for the whole Barnes–Hut stage. Warps first take the root pair
+// of each loop pair from a counter; later work comes from a ring of batches
+// that busy warps fill when other warps are waiting (they hand over the
+// older half of their stack). When the last batch of a pass of a loop pair
+// finishes, the warp that finished it reads the pair's sums and either
+// writes the result or queues the pair's next pass on the device: the
+// reference's beta retry (lnc.cpp:165-184), then up to bh_escalations
+// doublings of beta while the scaled estimate exceeds bh_err_limit. Every
+// wait is bounded; a wait that runs out sets status bit 1 and the host reruns
+// the stage with budgeted rounds.
+constexpr int kRing = 1 << 16;                 // batches in the ring
+// Queue counters on separate 128-byte lines (waiting warps poll kQLeft).
+constexpr int kQRoot = 0, kQHead = 16, kQTail = 32, kQLeft = 48, kQWords = 64;
+constexpr long long kWaitPolls = 1LL << 21;    // bounded wait (nanosleep backoff to 2 us: a few seconds)
+
+struct PersistArgs {
+  const double *xyz;
+  const int64_t *off;
+  const int64_t *node_base;
+  const NodeHdr *hdr;
+  const NodeMom *mom;
+  const int32_t *slot_loops;   // 2 per slot
+  const int32_t *slot_pair;    // slot -> caller pair
+  int32_t nslots;
+  int32_t tree_kind;
+  double epssq, beta0, beta_limit, target_error, err_scale, err_limit;
+  int32_t escalations;
+  double *slot_itolsq;         // per slot, current pass
+  int32_t *slot_pass;          // 0 first, 1 retry, >= 1 escalations
+  int32_t *slot_left;          // unfinished batches of the current pass
+  unsigned long long *acc_lk, *acc_err;
+  Batch *ring;
+  unsigned long long *ready;   // per ring entry: index + 1 once written
+  unsigned long long *q;       // [kQRoot] root counter, [kQHead] head, [kQTail] tail, [kQLeft] outstanding
+  double *lk, *err;            // per caller pair (err scaled)
+  int32_t *flags;              // per caller pair
+  double *counts;              // [0] far, [1] leaf, [2] retried, [3] escalated
+  int2 *spill;
+  int32_t *status;
+};
+
+__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long *p) {
+  return *(const volatile unsigned long long *)p;
+}
+
+// Publishes batches of slot `slot` built from the first `total` entries of
+// (spill[0..nspill) ++ stack[0..top)); warp-wide. The ring slots are
+// reserved with a compare-and-swap that refuses while more than half the ring
+// is published but unclaimed, so entries are never overwritten before their
+// claimant reads them. Returns false (nothing published) when refused.
+__device__ bool publish(PersistArgs &A, int slot, int lane, const int2 *spill, const int2 *stack, int nspill,
+                        int total) {
+  const int nb = (total + 31) / 32;
+  unsigned long long t = 0;
+  int ok = 0;
+  if (lane == 0) {
+    for (int tries = 0; tries < 64; ++tries) {
+      t = ld_volatile(&A.q[kQTail]);
+      const long long unclaimed = (long long)(t + nb) - (long long)ld_volatile(&A.q[kQHead]);
+      if (unclaimed > kRing / 2) break;
+      if (atomicCAS(&A.q[kQTail], t, t + nb) == t) {
+        ok = 1;
+        break;
+      }
+    }
+    if (ok) {
+      atomicAdd(&A.slot_left[slot], nb);
+      atomicAdd(&A.q[kQLeft], (unsigned long long)nb);
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (!ok) return false;
+  t = __shfl_sync(0xffffffffu, t, 0);
+  for (int b = 0; b < nb; ++b) {
+    Batch &B = A.ring[(t + b) & (kRing - 1)];
+    const int e = 32 * b + lane;
+    if (e < total) B.pairs[lane] = e < nspill ? spill[e] : stack[e - nspill];
+    if (lane == 0) {
+      B.slot = slot;
+      B.count = min(32, total - 32 * b);
+    }
+  }
+  __threadfence();
+  __syncwarp();
+  for (int b = lane; b < nb; b += 32) atomicExch(&A.ready[(t + b) & (kRing - 1)], t + b + 1);
+  return true;
+}
+
+// Called by the warp that finished the last batch of a pass of `slot`.
+__device__ void finish_pass(PersistArgs &A, int slot, int lane) {
+  if (lane != 0) return;
+  __threadfence();
+  const double lk = (double)(long long)atomicAdd(&A.acc_lk[slot], 0ULL) / kFix;
+  const double e = (double)(long long)atomicAdd(&A.acc_err[slot], 0ULL) / kFix * A.err_scale;
+  const int pass = A.slot_pass[slot];
+  const double beta = sqrt(A.slot_itolsq[slot]);
+  const int p = A.slot_pair[slot];
+  const int escalated = pass - ((A.flags[p] & FLN_PAIR_BETA_RETRIED) ? 1 : 0);
+  double next = 0.0;
+  int flag = 0;
+  if (pass == 0) {
+    const double tb = fmin(pow(e / A.target_error, 0.25) * A.beta0, A.beta_limit);
+    if (tb > A.beta0) {
+      next = tb;
+      flag = FLN_PAIR_BETA_RETRIED;
+    }
+  }
+  if (next == 0.0 && !(e <= A.err_limit) && escalated < A.escalations && beta < 4.0 * A.beta_limit) {
+    next = fmin(2.0 * beta, 4.0 * A.beta_limit);
+    flag = FLN_PAIR_BETA_ESCALATED;
+  }
+  if (next == 0.0) {
+    A.lk[p] = lk;
+    A.err[p] = e;
+    return;
+  }
+  // Queue the next pass of this pair.
+  A.flags[p] |= flag;
+  atomicAdd(A.counts + (flag == FLN_PAIR_BETA_RETRIED ? 2 : 3), 1.0);
+  A.slot_itolsq[slot] = next * next;
+  A.slot_pass[slot] = pass + 1;
+  A.acc_lk[slot] = 0;
+  A.acc_err[slot] = 0;
+  A.slot_left[slot] = 1;
+  atomicAdd(&A.q[kQLeft], 1ULL);
+  const unsigned long long t = atomicAdd(&A.q[kQTail], 1ULL);
+  Batch &B = A.ring[t & (kRing - 1)];
+  const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+  const int64_t n1 = A.off[l1 + 1] - A.off[l1], n2 = A.off[l2 + 1] - A.off[l2];
+  B.slot = slot;
+  B.count = 1;
+  B.pairs[0] = A.tree_kind == 0 ? make_int2((int)(n1 / 2 - 1), (int)(n2 / 2 - 1))
+                                : make_int2((int)(n1 - 2), (int)(n2 - 2));
+  __threadfence();
+  atomicExch(&A.ready[t & (kRing - 1)], t + 1);
+}
+
+__global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
+  __shared__ int2 s_stack[kWarps][kStack];
+  __shared__ int2 s_far[kWarps][64];
+  __shared__ int2 s_leaf[kWarps][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + w;
+  const int nwarps = gridDim.x * kWarps;
+  int2 *stack = s_stack[w];
+  int2 *farq = s_far[w];
+  int2 *leafq = s_leaf[w];
+  int2 *spill = A.spill + (size_t)gw * kSpill;
+  double nfar = 0, nleaf = 0;
+  bool quit = false;
+  while (!quit) {
+    // ---- take a batch: a root, else the next ring entry (bounded wait)
+    int slot = -1, cnt0 = 0;
+    unsigned long long h = 0;
+    bool from_ring = false;
+    if (lane == 0) {
+      if (ld_volatile(&A.q[kQRoot]) < (unsigned long long)A.nslots) {
+        const unsigned long long r = atomicAdd(&A.q[kQRoot], 1ULL);
+        if (r < (unsigned long long)A.nslots) slot = (int)r;
+      }
+      if (slot < 0) {
+        from_ring = true;
+        h = atomicAdd(&A.q[kQHead], 1ULL);
+        unsigned ns = 256;
+        long long polls = 0;
+        while (true) {
+          if (ld_volatile(&A.ready[h & (kRing - 1)]) == h + 1) break;
+          if ((polls & 15) == 15 && ld_volatile(&A.q[kQLeft]) == 0) {
+            slot = -2;  // all work done
+            break;
+          }
+          if (++polls > kWaitPolls) {
+            atomicOr(A.status, 2);
+            slot = -2;
+            break;
+          }
+          __nanosleep(ns);
+          if (ns < 2048) ns *= 2;
+        }
+        if (slot != -2) {
+          __threadfence();
+          slot = __ldcg(&A.ring[h & (kRing - 1)].slot);
+          cnt0 = __ldcg(&A.ring[h & (kRing - 1)].count);
+        }
+      } else {
+        cnt0 = 1;
+      }
+    }
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    cnt0 = __shfl_sync(0xffffffffu, cnt0, 0);
+    from_ring = __shfl_sync(0xffffffffu, from_ring, 0);
+    h = __shfl_sync(0xffffffffu, h, 0);
+    if (slot == -2) break;
+    const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+    const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
+    const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
+    const NodeMom *M1 = A.mom + A.node_base[l1], *M2 = A.mom + A.node_base[l2];
+    const double itolsq = __ldcg(&A.slot_itolsq[slot]), eps = A.epssq;
+    if (from_ring) {
+      if (lane < cnt0) {
+        const int2 *src = A.ring[h & (kRing - 1)].pairs;
+        stack[lane] = make_int2(__ldcg(&src[lane].x), __ldcg(&src[lane].y));
+      }
+    } else if (lane == 0) {
+      stack[0] = A.tree_kind == 0 ? make_int2((int)(n1 / 2 - 1), (int)(n2 / 2 - 1))
+                                  : make_int2((int)(n1 - 2), (int)(n2 - 2));
+    }
+    int top = cnt0, nspill = 0, nf = 0, nl = 0, steps = 0;
+    bool overflow = false;
+    double sum = 0.0, err = 0.0;
+    __syncwarp();
+    while (true) {
+      if (top == 0 && nspill > 0) {
+        const int k = min(nspill, kStack / 2);
+        for (int x = lane; x < k; x += 32) stack[x] = spill[nspill - k + x];
+        nspill -= k;
+        top = k;
+        __syncwarp();
+      }
+      if (top == 0) break;
+      // Hand the older half of the stack to waiting warps.
+      if ((++steps & 7) == 0 && top + nspill >= 64) {
+        long long waiting = 0;
+        if (lane == 0) waiting = (long long)(ld_volatile(&A.q[kQHead]) - ld_volatile(&A.q[kQTail]));
+        waiting = __shfl_sync(0xffffffffu, waiting, 0);
+        if (waiting > 0 && waiting <= nwarps) {
+          const int total = top + nspill;
+          const long long want = waiting > 8 ? 8 : waiting;
+          const int give = min(total / 2, 32 * (int)want);
+          if (publish(A, slot, lane, spill, stack, nspill, give)) {
+          // Drop the handed-over entries: they were the oldest (spill first).
+          // Shifts read a pass of 32 before writing it; earlier passes only
+          // wrote below what later passes read.
+          const int from_spill = min(give, nspill);
+          for (int base = 0; base < nspill - from_spill; base += 32) {
+            const int x = base + lane;
+            int2 v = make_int2(0, 0);
+            if (x < nspill - from_spill) v = spill[from_spill + x];
+            __syncwarp();
+            if (x < nspill - from_spill) spill[x] = v;
+            __syncwarp();
+          }
+          nspill -= from_spill;
+          const int from_stack = give - from_spill;
+          for (int base = 0; from_stack > 0 && base < top - from_stack; base += 32) {
+            const int x = base + lane;
+            int2 v = make_int2(0, 0);
+            if (x < top - from_stack) v = stack[from_stack + x];
+            __syncwarp();
+            if (x < top - from_stack) stack[x] = v;
+            __syncwarp();
+          }
+          top -= from_stack;
+          __syncwarp();
+          if (top == 0 && nspill == 0) break;
+          if (top == 0) continue;
+          }
+        }
+      }
+      const int cnt = min(top, 32);
+      const bool act = lane < cnt;
+      int2 pr = make_int2(0, 0);
+      if (act) pr = stack[top - cnt + lane];
+      __syncwarp();
+      top -= cnt;
+      int kind = 0;
+      int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
+      if (act) {
+        const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+        const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
+        const double rs = h1.r + h2.r;
+        if (leaf1 && leaf2) {
+          kind = 1;
+        } else if (dx * dx + dy * dy + dz * dz + eps > rs * rs * itolsq + eps) {
+          kind = 2;
+        } else {
+          kind = 3;
+          const bool split2 = (!leaf1 && !leaf2) ? (h2.rsq > h1.rsq) : !leaf2;
+          if (split2) {
+            c0 = make_int2(pr.x, h2.left);
+            c1 = make_int2(pr.x, h2.right);
+          } else {
+            c0 = make_int2(h1.left, pr.y);
+            c1 = make_int2(h1.right, pr.y);
+          }
+        }
+      }
+      const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
+      const int ns = __popc(sm);
+      if (top + 2 * ns > kStack) {
+        const int k = top / 2;
+        if (nspill + k > kSpill) {
+          overflow = true;
+          break;
+        }
+        for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
+        __syncwarp();
+        for (int x = lane; x < top - k; x += 32) stack[x] = stack[k + x];
+        nspill += k;
+        top -= k;
+        __syncwarp();
+      }
+      if (kind == 3) {
+        const int rank = __popc(sm & ((1u << lane) - 1));
+        stack[top + 2 * rank] = c0;
+        stack[top + 2 * rank + 1] = c1;
+      }
+      top += 2 * ns;
+      const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
+      const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
+      if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
+      if (kind == 1) leafq[nl + __popc(lm & ((1u << lane) - 1))] = pr;
+      nf += __popc(fm);
+      nl += __popc(lm);
+      __syncwarp();
+      while (nf >= 32) {
+        const int2 q = farq[nf - 32 + lane];
+        const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+        far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
+                 (float)h1.r, (float)h2.r, sum, err);
+        nfar += 32;
+        nf -= 32;
+        __syncwarp();
+      }
+      while (nl >= 32) {
+        const int2 q = leafq[nl - 32 + lane];
+        leaf_eval(A.xyz, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+        nleaf += 32;
+        nl -= 32;
+        __syncwarp();
+      }
+    }
+    if (lane < nf) {
+      const int2 q = farq[lane];
+      const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+      const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+      far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
+               (float)h2.r, sum, err);
+    }
+    if (lane < nl) {
+      const int2 q = leafq[lane];
+      leaf_eval(A.xyz, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+    }
+    nfar += nf;
+    nleaf += nl;
+    __syncwarp();
+    if (overflow && lane == 0) atomicOr(A.status, 1);
+    for (int o = 16; o; o >>= 1) {
+      sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      err += __shfl_xor_sync(0xffffffffu, err, o);
+    }
+    int last = 0;
+    if (lane == 0) {
+      fix_add(A.acc_lk + slot, sum);
+      fix_add(A.acc_err + slot, err);
+      __threadfence();
+      last = atomicSub(&A.slot_left[slot], 1) == 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) finish_pass(A, slot, lane);
+    if (lane == 0) {
+      __threadfence();
+      atomicAdd(&A.q[kQLeft], ~0ULL);  // -1
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    atomicAdd(A.counts, nfar);
+    atomicAdd(A.counts + 1, nleaf);
+  }
 }
 
 __global__ void scatter_kernel(const double *src, const int32_t *idx, int64_t n, double *dst) {
@@ -825,7 +1200,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   int32_t *d_slot_pair = d_slots + 2 * np;
   int32_t *d_active = d_slots + 3 * np;
   double *d_itol = ctx.d_bh[12].as<double>(np);
-  double *d_counts = ctx.d_bh[13].as<double>(2);
+  double *d_counts = ctx.d_bh[13].as<double>(8);  // far, leaf, retried, escalated, status words
   int32_t *d_status = reinterpret_cast<int32_t *>(d_counts + 2);
   unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(2 * np + 4);
   unsigned long long *d_acc_err = d_acc + np;
@@ -873,6 +1248,66 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       cur = 1 - cur;
     }
   };
+  // bh_schedule = 1: one persistent launch (retry and escalation on the
+  // device). The budgeted rounds below are the default and the fallback when
+  // a bounded wait of the persistent kernel runs out.
+  if (prm.bh_schedule == 1) {
+    double *d_sitol = ctx.d_bh[12].as<double>(np);
+    int32_t *d_sint = reinterpret_cast<int32_t *>(ctx.d_near.need((size_t)np * 2 * sizeof(int32_t) + 64));
+    int32_t *d_pass_arr = d_sint, *d_left = d_sint + np;
+    unsigned long long *d_ready = reinterpret_cast<unsigned long long *>(
+        ctx.d_items.need((size_t)(kRing + kQWords) * sizeof(unsigned long long)));
+    unsigned long long *d_q = d_ready + kRing;
+    Batch *d_ring = reinterpret_cast<Batch *>(ctx.d_partial.need((size_t)kRing * sizeof(Batch)));
+    int32_t *d_fl = d_flags_out ? d_flags_out : reinterpret_cast<int32_t *>(ctx.d_flags.need(np * sizeof(int32_t)));
+    double *d_cnt4 = d_counts;  // [0] far [1] leaf [2] retried [3] escalated [4] status
+    d_status = reinterpret_cast<int32_t *>(d_cnt4 + 4);
+    std::vector<double> itol0(np, b0 * b0);
+    std::vector<int32_t> ones(np, 1);
+    unsigned long long q0[kQWords] = {0};
+    q0[kQLeft] = (unsigned long long)np;
+    FLN_CUDA(cudaMemcpyAsync(d_sitol, itol0.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemsetAsync(d_pass_arr, 0, np * sizeof(int32_t), st));
+    FLN_CUDA(cudaMemcpyAsync(d_left, ones.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemsetAsync(d_acc, 0, 2 * np * sizeof(unsigned long long), st));
+    FLN_CUDA(cudaMemsetAsync(d_ready, 0, kRing * sizeof(unsigned long long), st));
+    FLN_CUDA(cudaMemcpyAsync(d_q, q0, sizeof q0, cudaMemcpyHostToDevice, st));
+    FLN_CUDA(cudaMemsetAsync(d_fl, 0, np * sizeof(int32_t), st));
+    FLN_CUDA(cudaMemsetAsync(d_cnt4, 0, 4 * sizeof(double) + sizeof(int32_t), st));
+    PersistArgs P{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_slot_pair, (int32_t)np, prm.bh_tree == 1 ? 1 : 0,
+                  prm.epssq, b0, prm.barnes_hut_beta_limit, prm.target_error, prm.error_est_scale,
+                  prm.bh_err_limit, prm.bh_escalations, d_sitol, d_pass_arr, d_left, d_acc, d_acc_err, d_ring,
+                  d_ready, d_q, d_lk_out, d_err_out, d_fl, d_cnt4, d_spill, d_status};
+    int per_sm_p = 0;
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, bh_persistent, 32 * kWarps, 0));
+    const int gp = std::min(grid, ctx.num_sms * std::max(per_sm_p, 1));
+    FLN_CUDA(cudaEventRecord(ctx.ev2, st));
+    bh_persistent<<<gp, 32 * kWarps, 0, st>>>(P);
+    FLN_CUDA(cudaGetLastError());
+    FLN_CUDA(cudaEventRecord(ctx.ev3, st));
+    ++launches;
+    ctx.stats.bh_rounds = 1;
+    double cnt[4];
+    int32_t pst = 0;
+    FLN_CUDA(cudaMemcpyAsync(cnt, d_cnt4, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaMemcpyAsync(&pst, d_status, sizeof pst, cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+    ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+    if (pst & 1)
+      throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
+                                              std::to_string(maxdepth) + ").");
+    if (!(pst & 2)) {
+      ctx.stats.bh_far_evals = cnt[0];
+      ctx.stats.bh_leaf_evals = cnt[1];
+      ctx.stats.beta_retried = (int64_t)cnt[2];
+      ctx.stats.bh_escalated = (int64_t)cnt[3];
+      return launches;
+    }
+    // A bounded wait ran out: redo the stage with budgeted rounds.
+    ctx.stats.bh_wait_timeouts += 1;
+    d_status = reinterpret_cast<int32_t *>(d_counts + 2);
+    FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
+  }
   std::vector<int32_t> all(np);
   std::iota(all.begin(), all.end(), 0);
   std::vector<double> itol(np, b0 * b0);

@@ -83,7 +83,9 @@ typedef struct fln_params {
                                    above bh_err_limit is re-run with twice its beta, up to this many times;
                                    default 2 (0 = the reference's behaviour) */
   double bh_err_limit;          /* default 0.25; a pair still above it is recomputed by FP64 direct sum */
-  int32_t reserved[4];
+  int32_t bh_schedule;          /* 0 = budgeted rounds, one launch per round (default);
+                                   1 = one persistent launch with a device work queue */
+  int32_t reserved[3];
 } fln_params;
 
 /* Statistics of the last computation on a context. */
@@ -107,6 +109,7 @@ typedef struct fln_stats {
   int32_t bh_rounds;            /* Barnes–Hut traversal launches (work is handed on between rounds) */
   int32_t reserved_stats;
   int64_t bh_escalated;         /* pair re-runs with an escalated beta */
+  int64_t bh_wait_timeouts;     /* persistent traversals that fell back to rounds */
 } fln_stats;
 
 typedef struct fln_ctx fln_ctx;

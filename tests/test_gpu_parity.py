@@ -200,3 +200,19 @@ def test_device_pointer_entry(engine):
                                   len(pairs), d_lk.data_ptr(), method="directsum")
     host, _, _ = engine.linking_numbers(xyz, off, pairs, "directsum")
     np.testing.assert_allclose(d_lk.cpu().numpy(), host, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["knittubebroken", "glove"])
+def test_persistent_and_round_schedules_agree(engine, name, golden_dir):
+    # The budgeted rounds (default) and the persistent work queue evaluate the
+    # same node pairs; only the grouping of FP64 partial sums differs.
+    _, off, xyz, pairs = _prepared(name, golden_dir)
+    lk0, err0, fl0 = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=0)
+    s0 = engine.stats()
+    lk1, err1, fl1 = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=1)
+    s1 = engine.stats()
+    np.testing.assert_allclose(lk0, lk1, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(err0, err1, rtol=1e-9, atol=1e-12)
+    assert np.array_equal(fl0, fl1)
+    assert s0["bh_far_evals"] == s1["bh_far_evals"] and s0["bh_leaf_evals"] == s1["bh_leaf_evals"]
+    assert s1["bh_wait_timeouts"] == 0
