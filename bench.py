@@ -275,7 +275,7 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(cfg, parallelism=f"replicas x{world}"),
         "impl_details": {"method": args.method, "precision": args.precision,
                          "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median",
-                         "schedule": "budgeted rounds" if args.bh_schedule == 0 else "persistent queue"},
+                         "schedule": ["rounds, fused evaluation", "persistent queue", "rounds, split evaluation"][args.bh_schedule]},
         "certificate_ms": ms,
         "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(pxyz.nbytes + poff.nbytes + pairs.nbytes),
@@ -329,7 +329,7 @@ def main():
     ap.add_argument("--method", default="barneshut", choices=["barneshut", "directsum"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--bh-tree", type=int, default=0)
-    ap.add_argument("--bh-schedule", type=int, default=0, help="0 budgeted rounds, 1 persistent queue")
+    ap.add_argument("--bh-schedule", type=int, default=0, help="0 rounds (fused evaluation), 1 persistent queue, 2 rounds (split evaluation)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--loops", type=int, default=200)
     ap.add_argument("--loop-steps", type=int, default=50000)

@@ -51,6 +51,9 @@ constexpr double kInvRt3 = 0.57735026918962576450914878050195746;
 constexpr int kWarps = 4;          // warps per traversal CTA
 constexpr int kStack = 512;        // shared-memory stack entries per warp
 constexpr int kSpill = 8192;       // global spill entries per warp
+#ifndef FLN_CHUNK_SOFT_LOG2
+#define FLN_CHUNK_SOFT_LOG2 20  // chunks per list before a round stops taking batches
+#endif
 
 // FP64 build record.
 struct BuildNode {
@@ -618,6 +621,259 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
   if (lane == 0) {
     atomicAdd(A.counts, nfar);
     atomicAdd(A.counts + 1, nleaf);
+  }
+}
+
+// ------------------------------------------------------------------ split evaluation
+// Rounds with the evaluation taken out of the traversal: bh_classify walks
+// the trees and writes far-field and leaf node pairs as chunks of up to 32
+// (one loop pair per chunk); bh_far_chunks and bh_leaf_chunks evaluate them.
+// The traversal then needs few registers (more warps per SM to cover its
+// dependent loads) and the evaluation runs as streaming kernels with full
+// warps and one fixed-point atomic per chunk.
+struct Chunk {
+  int32_t slot;
+  int32_t count;
+  int2 pairs[32];
+};
+
+struct ClassifyArgs {
+  const int64_t *off;
+  const int64_t *node_base;
+  const NodeHdr *hdr;
+  const int32_t *slot_loops;
+  const double *itolsq;
+  double epssq;
+  const Batch *in;
+  int64_t nin;
+  Batch *out;
+  int64_t out_cap;
+  unsigned long long *out_count;
+  int32_t budget;
+  Chunk *far_chunks, *leaf_chunks;
+  unsigned long long *far_count, *leaf_count;  // chunks written
+  int64_t chunk_soft, chunk_cap;                // stop taking batches past soft; hard capacity
+  int2 *spill;
+  unsigned long long *queue;
+  int32_t *status;                              // bit 0 stack overflow, bit 2 chunk capacity
+};
+
+__device__ __forceinline__ void flush_chunk(Chunk *list, unsigned long long *count, int64_t cap, int slot,
+                                            const int2 *q, int n, int lane, int32_t *status) {
+  unsigned long long c = 0;
+  if (lane == 0) c = atomicAdd(count, 1ULL);
+  c = __shfl_sync(0xffffffffu, c, 0);
+  if ((int64_t)c >= cap) {
+    if (lane == 0) atomicOr(status, 4);
+    return;
+  }
+  if (lane < n) list[c].pairs[lane] = q[lane];
+  if (lane == 0) {
+    list[c].slot = slot;
+    list[c].count = n;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kWarps) bh_classify(ClassifyArgs A) {
+  __shared__ int2 s_stack[kWarps][kStack];
+  __shared__ int2 s_far[kWarps][64];
+  __shared__ int2 s_leaf[kWarps][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + w;
+  int2 *stack = s_stack[w];
+  int2 *farq = s_far[w];
+  int2 *leafq = s_leaf[w];
+  int2 *spill = A.spill + (size_t)gw * kSpill;
+  for (;;) {
+    long long b = 0;
+    if (lane == 0) {
+      // Past the soft limit this round takes no new batch (they carry over).
+      const bool full = (int64_t)*(volatile unsigned long long *)A.far_count > A.chunk_soft ||
+                        (int64_t)*(volatile unsigned long long *)A.leaf_count > A.chunk_soft;
+      b = full ? A.nin : (long long)atomicAdd(A.queue, 1ULL);
+    }
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (b >= A.nin) break;
+    const int slot = A.in[b].slot;
+    const int cnt0 = A.in[b].count;
+    const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+    const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
+    const double itolsq = A.itolsq[slot], eps = A.epssq;
+    if (lane < cnt0) stack[lane] = A.in[b].pairs[lane];
+    int top = cnt0, nspill = 0, nf = 0, nl = 0, steps = 0;
+    bool overflow = false;
+    __syncwarp();
+    while (true) {
+      if (top == 0 && nspill > 0) {
+        const int k = min(nspill, kStack / 2);
+        for (int x = lane; x < k; x += 32) stack[x] = spill[nspill - k + x];
+        nspill -= k;
+        top = k;
+        __syncwarp();
+      }
+      if (top == 0) break;
+      if (steps >= A.budget) {
+        const int total = top + nspill;
+        const int nb = (total + 31) / 32;
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(A.out_count, (unsigned long long)nb);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if ((long long)(at + nb) <= A.out_cap) {
+          for (int q = 0; q < nb; ++q) {
+            const int e = 32 * q + lane;
+            if (e < total) A.out[at + q].pairs[lane] = e < nspill ? spill[e] : stack[e - nspill];
+            if (lane == 0) {
+              A.out[at + q].slot = slot;
+              A.out[at + q].count = min(32, total - 32 * q);
+            }
+          }
+          top = 0;
+          nspill = 0;
+          __syncwarp();
+          break;
+        }
+        if (lane == 0)
+          for (int q = 0; q < nb && (long long)(at + q) < A.out_cap; ++q) {
+            A.out[at + q].slot = slot;
+            A.out[at + q].count = 0;
+          }
+        steps = INT_MIN;
+      }
+      ++steps;
+      const int cnt = min(top, 32);
+      const bool act = lane < cnt;
+      int2 pr = make_int2(0, 0);
+      if (act) pr = stack[top - cnt + lane];
+      __syncwarp();
+      top -= cnt;
+      int kind = 0;
+      int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
+      if (act) {
+        const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+        const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
+        const double rs = h1.r + h2.r;
+        if (leaf1 && leaf2) {
+          kind = 1;
+        } else if (dx * dx + dy * dy + dz * dz + eps > rs * rs * itolsq + eps) {
+          kind = 2;
+        } else {
+          kind = 3;
+          const bool split2 = (!leaf1 && !leaf2) ? (h2.rsq > h1.rsq) : !leaf2;
+          if (split2) {
+            c0 = make_int2(pr.x, h2.left);
+            c1 = make_int2(pr.x, h2.right);
+          } else {
+            c0 = make_int2(h1.left, pr.y);
+            c1 = make_int2(h1.right, pr.y);
+          }
+        }
+      }
+      const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
+      const int ns = __popc(sm);
+      if (top + 2 * ns > kStack) {
+        const int k = top / 2;
+        if (nspill + k > kSpill) {
+          overflow = true;
+          break;
+        }
+        for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
+        __syncwarp();
+        for (int x = lane; x < top - k; x += 32) stack[x] = stack[k + x];
+        nspill += k;
+        top -= k;
+        __syncwarp();
+      }
+      if (kind == 3) {
+        const int rank = __popc(sm & ((1u << lane) - 1));
+        stack[top + 2 * rank] = c0;
+        stack[top + 2 * rank + 1] = c1;
+      }
+      top += 2 * ns;
+      const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
+      const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
+      if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
+      if (kind == 1) leafq[nl + __popc(lm & ((1u << lane) - 1))] = pr;
+      nf += __popc(fm);
+      nl += __popc(lm);
+      __syncwarp();
+      if (nf >= 32) {
+        flush_chunk(A.far_chunks, A.far_count, A.chunk_cap, slot, farq + nf - 32, 32, lane, A.status);
+        nf -= 32;
+        __syncwarp();
+      }
+      if (nl >= 32) {
+        flush_chunk(A.leaf_chunks, A.leaf_count, A.chunk_cap, slot, leafq + nl - 32, 32, lane, A.status);
+        nl -= 32;
+        __syncwarp();
+      }
+    }
+    if (nf > 0) flush_chunk(A.far_chunks, A.far_count, A.chunk_cap, slot, farq, nf, lane, A.status);
+    if (nl > 0) flush_chunk(A.leaf_chunks, A.leaf_count, A.chunk_cap, slot, leafq, nl, lane, A.status);
+    __syncwarp();
+    if (overflow && lane == 0) atomicOr(A.status, 1);
+  }
+}
+
+struct EvalArgs {
+  const double *xyz;
+  const int64_t *off;
+  const int64_t *node_base;
+  const NodeHdr *hdr;
+  const NodeMom *mom;
+  const int32_t *slot_loops;
+  double epssq;
+  const Chunk *chunks;
+  int64_t nchunks;
+  unsigned long long *acc_lk, *acc_err;
+  double *count;  // evaluations
+};
+
+// One warp per chunk of far-field node pairs.
+__global__ void __launch_bounds__(256) bh_far_chunks(EvalArgs A) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c >= A.nchunks) return;
+  const int slot = A.chunks[c].slot, n = A.chunks[c].count;
+  const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+  const int64_t b1 = A.node_base[l1], b2 = A.node_base[l2];
+  double sum = 0.0, err = 0.0;
+  if (lane < n) {
+    const int2 q = A.chunks[c].pairs[lane];
+    const NodeHdr h1 = A.hdr[b1 + q.x], h2 = A.hdr[b2 + q.y];
+    const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+    far_eval(A.mom[b1 + q.x], A.mom[b2 + q.y], (float)dx, (float)dy, (float)dz,
+             dx * dx + dy * dy + dz * dz + A.epssq, (float)h1.r, (float)h2.r, sum, err);
+  }
+  for (int o = 16; o; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    err += __shfl_xor_sync(0xffffffffu, err, o);
+  }
+  if (lane == 0) {
+    fix_add(A.acc_lk + slot, sum);
+    fix_add(A.acc_err + slot, err);
+    atomicAdd(A.count, (double)n);
+  }
+}
+
+// One warp per chunk of leaf-leaf segment pairs.
+__global__ void __launch_bounds__(256) bh_leaf_chunks(EvalArgs A) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c >= A.nchunks) return;
+  const int slot = A.chunks[c].slot, n = A.chunks[c].count;
+  const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+  const int64_t b1 = A.node_base[l1], b2 = A.node_base[l2];
+  const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
+  double sum = 0.0;
+  if (lane < n) {
+    const int2 q = A.chunks[c].pairs[lane];
+    leaf_eval(A.xyz, A.hdr[b1 + q.x], A.hdr[b2 + q.y], A.mom[b1 + q.x], A.mom[b2 + q.y], o1, n1, o2, n2, sum);
+  }
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0) {
+    fix_add(A.acc_lk + slot, sum);
+    atomicAdd(A.count, (double)n);
   }
 }
 
@@ -1202,15 +1458,19 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   double *d_itol = ctx.d_bh[12].as<double>(np);
   double *d_counts = ctx.d_bh[13].as<double>(8);  // far, leaf, retried, escalated, status words
   int32_t *d_status = reinterpret_cast<int32_t *>(d_counts + 2);
-  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(2 * np + 4);
+  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(2 * np + 8);
   unsigned long long *d_acc_err = d_acc + np;
-  unsigned long long *d_ctr = d_acc + 2 * np;  // [0] queue, [1] next-round count
+  unsigned long long *d_ctr = d_acc + 2 * np;  // [0] queue, [1] next-round count, [2] far chunks, [3] leaf chunks
   int per_sm = 0;
   FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_traverse, 32 * kWarps, 0));
   per_sm = std::max(per_sm, 1);
   const int grid = ctx.num_sms * per_sm;
   const int64_t nwarps = (int64_t)grid * kWarps;
-  int2 *d_spill = ctx.d_bh[14].as<int2>((size_t)nwarps * kSpill);
+  int per_sm_c = 0;
+  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, bh_classify, 32 * kWarps, 0));
+  const int grid_c = ctx.num_sms * std::max(per_sm_c, 1);
+  const int64_t nwarps_c = (int64_t)grid_c * kWarps;
+  int2 *d_spill = ctx.d_bh[14].as<int2>((size_t)std::max(nwarps, nwarps_c) * kSpill);
   // Round buffers: a warp hands on at most (kStack + kSpill) / 32 + 1 batches.
   const int64_t cap = std::max<int64_t>(np, nwarps * ((kStack + kSpill) / 32 + 1));
   Batch *d_batch[2] = {reinterpret_cast<Batch *>(ctx.d_partial.need(2 * cap * sizeof(Batch))), nullptr};
@@ -1220,6 +1480,15 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
   const double b0 = prm.barnes_hut_init_beta;
   const int budget = 256;
+  // Chunk lists of the split evaluation: a warp can write at most budget + 2
+  // chunks per list after the soft limit stops new batches.
+  const int64_t chunk_soft = int64_t(1) << FLN_CHUNK_SOFT_LOG2;
+  const int64_t chunk_cap = chunk_soft + std::max(nwarps, nwarps_c) * (budget + 2);
+  Chunk *d_far = nullptr, *d_leaf = nullptr;
+  if (prm.bh_schedule == 2) {
+    d_far = reinterpret_cast<Chunk *>(ctx.d_bh[16].need((size_t)chunk_cap * sizeof(Chunk)));
+    d_leaf = reinterpret_cast<Chunk *>(ctx.d_bh[17].need((size_t)chunk_cap * sizeof(Chunk)));
+  }
   ctx.stats.bh_rounds = 0;
   // One Barnes–Hut pass over the slots in `active` with per-slot beta^2.
   auto pass = [&](const std::vector<int32_t> &active, const std::vector<double> &itol_slots) {
@@ -1233,7 +1502,43 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     int64_t nin = na;
     int cur = 0;
     for (int round = 0; nin > 0 && round < 4096; ++round) {
-      FLN_CUDA(cudaMemsetAsync(d_ctr, 0, 2 * sizeof(unsigned long long), st));
+      FLN_CUDA(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
+      if (prm.bh_schedule == 2) {
+        // Classify, then evaluate this round's chunks.
+        ClassifyArgs C{d_off, d_base, d_hdr, d_slots, d_itol, prm.epssq, d_batch[cur], nin, d_batch[1 - cur], cap,
+                       d_ctr + 1, budget, d_far, d_leaf, d_ctr + 2, d_ctr + 3, chunk_soft, chunk_cap, d_spill,
+                       d_ctr, d_status};
+        const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, grid_c));
+        bh_classify<<<g, 32 * kWarps, 0, st>>>(C);
+        FLN_CUDA(cudaGetLastError());
+        unsigned long long c4[4];
+        FLN_CUDA(cudaMemcpyAsync(c4, d_ctr, sizeof c4, cudaMemcpyDeviceToHost, st));
+        FLN_CUDA(cudaStreamSynchronize(st));
+        const int64_t nfar = (int64_t)std::min<unsigned long long>(c4[2], (unsigned long long)chunk_cap);
+        const int64_t nleaf = (int64_t)std::min<unsigned long long>(c4[3], (unsigned long long)chunk_cap);
+        EvalArgs E{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, prm.epssq, d_far, nfar, d_acc, d_acc_err, d_counts};
+        if (nfar > 0) bh_far_chunks<<<(int)((nfar * 32 + 255) / 256), 256, 0, st>>>(E);
+        E.chunks = d_leaf;
+        E.nchunks = nleaf;
+        E.count = d_counts + 1;
+        if (nleaf > 0) bh_leaf_chunks<<<(int)((nleaf * 32 + 255) / 256), 256, 0, st>>>(E);
+        FLN_CUDA(cudaGetLastError());
+        launches += 3;
+        ++ctx.stats.bh_rounds;
+        // Batches not taken this round (past the chunk soft limit) carry over.
+        int64_t next = (int64_t)std::min<unsigned long long>(c4[1], (unsigned long long)cap);
+        const int64_t taken = (int64_t)std::min<unsigned long long>(c4[0], (unsigned long long)nin);
+        if (taken < nin) {
+          const int64_t keep = std::min<int64_t>(nin - taken, cap - next);
+          FLN_CUDA(cudaMemcpyAsync(d_batch[1 - cur] + next, d_batch[cur] + taken, keep * sizeof(Batch),
+                                   cudaMemcpyDeviceToDevice, st));
+          if (keep < nin - taken) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut round buffer too small");
+          next += keep;
+        }
+        nin = next;
+        cur = 1 - cur;
+        continue;
+      }
       TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
                  d_batch[1 - cur], cap, d_ctr + 1, budget, d_acc, d_acc_err, d_counts, d_spill, d_ctr, d_status};
       const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, grid));

@@ -141,6 +141,7 @@ static fln_params resolved(const fln_params *p) {
   if (!(r.barnes_hut_init_beta > 0) || !(r.barnes_hut_beta_limit > 0))
     throw Error(FLN_ERR_INVALID_ARGUMENT, "Barnes-Hut beta must be positive");
   if (r.bh_escalations < 0 || r.bh_escalations > 8) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_escalations in [0, 8]");
+  if (r.bh_schedule < 0 || r.bh_schedule > 2) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_schedule in [0, 2]");
   return r;
 }
 

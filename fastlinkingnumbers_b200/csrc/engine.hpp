@@ -83,7 +83,7 @@ struct Context {
   fln_stats stats{};
   // Device buffers.
   DevBuf d_xyz, d_off, d_pairs, d_loops, d_items, d_partial, d_counter, d_lk, d_err, d_flags, d_near;
-  DevBuf d_bh[16];
+  DevBuf d_bh[24];
   HostBuf h_in, h_out;
 
   explicit Context(int dev, void *user_stream);

@@ -83,8 +83,9 @@ typedef struct fln_params {
                                    above bh_err_limit is re-run with twice its beta, up to this many times;
                                    default 2 (0 = the reference's behaviour) */
   double bh_err_limit;          /* default 0.25; a pair still above it is recomputed by FP64 direct sum */
-  int32_t bh_schedule;          /* 0 = budgeted rounds, one launch per round (default);
-                                   1 = one persistent launch with a device work queue */
+  int32_t bh_schedule;          /* 0 = budgeted rounds, evaluation inside the traversal (default);
+                                   1 = one persistent launch with a device work queue;
+                                   2 = budgeted rounds, evaluation in separate streaming kernels */
   int32_t reserved[3];
 } fln_params;
 

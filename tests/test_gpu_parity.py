@@ -203,16 +203,19 @@ def test_device_pointer_entry(engine):
 
 
 @pytest.mark.parametrize("name", ["knittubebroken", "glove"])
-def test_persistent_and_round_schedules_agree(engine, name, golden_dir):
-    # The budgeted rounds (default) and the persistent work queue evaluate the
-    # same node pairs; only the grouping of FP64 partial sums differs.
+def test_traversal_schedules_agree(engine, name, golden_dir):
+    # Fused rounds (default), the persistent work queue and the split-
+    # evaluation rounds evaluate the same node pairs; only the grouping of the
+    # FP64 partial sums differs.
     _, off, xyz, pairs = _prepared(name, golden_dir)
-    lk0, err0, fl0 = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=0)
-    s0 = engine.stats()
-    lk1, err1, fl1 = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=1)
-    s1 = engine.stats()
-    np.testing.assert_allclose(lk0, lk1, rtol=0, atol=1e-9)
-    np.testing.assert_allclose(err0, err1, rtol=1e-9, atol=1e-12)
-    assert np.array_equal(fl0, fl1)
-    assert s0["bh_far_evals"] == s1["bh_far_evals"] and s0["bh_leaf_evals"] == s1["bh_leaf_evals"]
-    assert s1["bh_wait_timeouts"] == 0
+    runs = []
+    for sched in (0, 1, 2):
+        lk, err, fl = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=sched)
+        runs.append((lk, err, fl, engine.stats()))
+    lk0, err0, fl0, s0 = runs[0]
+    for lk, err, fl, s in runs[1:]:
+        np.testing.assert_allclose(lk, lk0, rtol=0, atol=1e-9)
+        np.testing.assert_allclose(err, err0, rtol=1e-9, atol=1e-12)
+        assert np.array_equal(fl, fl0)
+        assert s["bh_far_evals"] == s0["bh_far_evals"] and s["bh_leaf_evals"] == s0["bh_leaf_evals"]
+        assert s["bh_wait_timeouts"] == 0
