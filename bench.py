@@ -305,6 +305,37 @@ def run_ours(args, rank, world, local_rank):
                          "extrapolated_certificate_ms": s["ms_main_kernel"] * units / w}
         result["direct_sum_sample"] = out
         result["speedup_vs_fp64_direct"] = out["fp64"]["extrapolated_certificate_ms"] / ms
+    if rank == 0 and world == 1 and args.learned_leg and args.method == "barneshut":
+        # The learned opening criterion, trained on another seed of the same
+        # workload family, on this workload: one step, against the plain one.
+        from fastlinkingnumbers_b200 import LearnedCriterion
+        t0 = time.perf_counter()
+        toff, txyz, tpairs, _ = make_workload(args.workload, args.seed + 1000, args.loops, args.loop_steps)
+        model = LearnedCriterion.train(eng, txyz, toff, tpairs, params=prm)
+        train_s = time.perf_counter() - t0
+        eng.set_learned(model)
+        try:
+            runs = []
+            for _ in range(2):
+                step()
+                runs.append((eng.stats(), d_lk.cpu().numpy()))
+        finally:
+            eng.set_learned(None)
+        sl, llk = min(runs, key=lambda r: r[0]["ms_kernels"])
+        info = model.info()
+        result["learned_leg"] = {
+            "trained_on": f"seed {args.seed + 1000} of the same workload family (held out)",
+            "train": {k: info[k] for k in ("recorded", "samples", "log10_tau", "s_min", "val_loss",
+                                           "val_coverage", "ms_collect", "ms_train")},
+            "train_wall_s_incl_workload": round(train_s, 2),
+            "certificate_ms": sl["ms_kernels"], "main_kernel_ms": sl["ms_main_kernel"],
+            "node_pairs": sl["bh_far_evals"] + sl["bh_leaf_evals"],
+            "plain_node_pairs": node_pairs, "plain_certificate_ms": ms,
+            "beta_retried": sl["beta_retried"], "escalated": sl["bh_escalated"],
+            "fp64_recomputed": sl["fp64_recomputed"],
+            "same_integers_as_plain": bool(np.array_equal(np.round(llk), np.round(lk))),
+            "max_abs_diff_vs_plain": float(np.abs(llk - lk).max()),
+        }
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         from oracle import pyoracle
         thr = pyoracle.max_threads()
@@ -336,6 +367,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
     ap.add_argument("--traffic-bytes", type=float, default=None)
+    ap.add_argument("--learned-leg", type=int, default=1,
+                    help="also train the learned opening criterion on another seed and time one step with it")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

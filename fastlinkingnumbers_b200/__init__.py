@@ -11,7 +11,9 @@ from .api import (  # noqa: F401
     ComputeLinkingNumberDirectFast,
     ComputeLinkingNumberDirectOneArctanPerPair,
     Engine,
+    LearnedCriterion,
     LinkingNumberCertificate,
     Model,
     default_engine,
+    learned_options,
 )

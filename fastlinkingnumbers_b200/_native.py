@@ -40,7 +40,12 @@ EXPORTED = [
     "fln_certificate_text", "fln_certificate_num_curves", "fln_certificate_num_entries",
     "fln_certificate_entries", "fln_certificate_num_pairs", "fln_certificate_pairs",
     "fln_certificate_equals", "fln_certificate_export_diffs",
+    "fln_learned_default_options", "fln_learned_train", "fln_learned_create", "fln_learned_destroy",
+    "fln_learned_get", "fln_ctx_set_learned", "fln_learned_collect", "fln_learned_predict",
+    "fln_learned_gradients",
 ]
+
+MLP_PARAMS = 4801  # FLN_MLP_PARAMS
 
 
 class Params(C.Structure):
@@ -67,6 +72,29 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LearnedOptions(C.Structure):
+    _fields_ = [
+        ("s_min", C.c_double), ("sample_keep", C.c_double), ("max_samples", C.c_int64),
+        ("max_terms", C.c_int64), ("epochs", C.c_int32), ("batch", C.c_int32),
+        ("learning_rate", C.c_double), ("quantile", C.c_double), ("tau_quantile", C.c_double),
+        ("val_fraction", C.c_double), ("min_candidates", C.c_int32), ("reserved0", C.c_int32),
+        ("seed", C.c_uint64), ("reserved", C.c_double * 4),
+    ]
+
+
+class LearnedInfo(C.Structure):
+    _fields_ = [
+        ("recorded", C.c_int64), ("samples", C.c_int64), ("train_samples", C.c_int64),
+        ("val_samples", C.c_int64), ("s_min", C.c_double), ("log10_tau", C.c_double),
+        ("min_candidates", C.c_int32), ("epochs", C.c_int32), ("train_loss", C.c_double),
+        ("val_loss", C.c_double), ("val_coverage", C.c_double), ("ms_collect", C.c_double),
+        ("ms_train", C.c_double), ("reserved", C.c_double * 4),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 class FlnError(RuntimeError):
@@ -134,6 +162,18 @@ def load():
     L.fln_certificate_equals.argtypes = [vp, vp]
     L.fln_certificate_equals.restype = C.c_int
     L.fln_certificate_export_diffs.argtypes = [vp, vp, C.c_char_p, C.c_char_p]
+    L.fln_learned_default_options.argtypes = [P(LearnedOptions)]
+    L.fln_learned_default_options.restype = None
+    L.fln_learned_train.argtypes = [vp, vp, vp, i32, vp, i64, P(Params), P(LearnedOptions), P(vp)]
+    L.fln_learned_create.argtypes = [vp, f64, f64, i32, P(vp)]
+    L.fln_learned_destroy.argtypes = [vp]
+    L.fln_learned_destroy.restype = None
+    L.fln_learned_get.argtypes = [vp, vp, P(LearnedInfo)]
+    L.fln_ctx_set_learned.argtypes = [vp, vp]
+    L.fln_learned_collect.argtypes = [vp, vp, vp, i32, vp, i64, P(Params), f64, f64, i64, i64, vp, vp,
+                                      vp, vp, P(i64)]
+    L.fln_learned_predict.argtypes = [vp, vp, vp, i64, i32, vp]
+    L.fln_learned_gradients.argtypes = [vp, vp, vp, vp, i64, f64, vp, P(f64)]
     _lib = L
     return L
 

@@ -89,6 +89,122 @@ class Engine:
                                         C.byref(out)))
         return out.value
 
+    # ---- learned opening criterion (no counterpart in the reference)
+    def set_learned(self, model: Optional["LearnedCriterion"]):
+        """Uses `model` for the Barnes–Hut opening decisions of this engine (None: off)."""
+        N.check(self._L.fln_ctx_set_learned(self._h, model.handle if model is not None else None))
+
+    def learned_collect(self, xyz, loop_offsets, pairs, cap: int, s_min: float = 1.0,
+                        sample_keep: float = 0.05, max_terms: int = 1 << 16,
+                        params: Optional[N.Params] = None, **overrides):
+        """Training samples the way LearnedCriterion.train records them:
+        (features (n, 8) float32, log10 true error (n,), separation (n,),
+        log10 of the scaled Eq. 14 estimate (n,))."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        off = np.ascontiguousarray(loop_offsets, dtype=np.int64)
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        prm = params if params is not None else default_params(**overrides)
+        X = np.zeros((max(cap, 1), 8), dtype=np.float32)
+        T = np.zeros(max(cap, 1), dtype=np.float32)
+        S = np.zeros(max(cap, 1), dtype=np.float32)
+        E = np.zeros(max(cap, 1), dtype=np.float32)
+        n = C.c_int64()
+        N.check(self._L.fln_learned_collect(
+            self._h, _ptr(xyz), _ptr(off), len(off) - 1, _ptr(pairs), len(pairs), C.byref(prm),
+            float(s_min), float(sample_keep), int(cap), int(max_terms), _ptr(X), _ptr(T), _ptr(S),
+            _ptr(E), C.byref(n)))
+        k = n.value
+        return X[:k].copy(), T[:k].copy(), S[:k].copy(), E[:k].copy()
+
+    def mlp_predict(self, params, features, use_mma: bool = False) -> np.ndarray:
+        """MLP outputs for rows of 8 features: FP32, or the traversal's BF16 warp-MMA path."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        X = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 8)
+        if p.size != N.MLP_PARAMS:
+            raise FlnError(1, f"expected {N.MLP_PARAMS} parameters")
+        y = np.zeros(len(X), dtype=np.float32)
+        N.check(self._L.fln_learned_predict(self._h, _ptr(p), _ptr(X), len(X), int(use_mma),
+                                            _ptr(y)))
+        return y
+
+    def mlp_gradients(self, params, features, targets, quantile: float = 0.9):
+        """(mean pinball loss, d loss / d params) from the training kernel."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        X = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 8)
+        T = np.ascontiguousarray(targets, dtype=np.float32).reshape(-1)
+        if p.size != N.MLP_PARAMS or len(T) != len(X):
+            raise FlnError(1, "parameter or row count")
+        g = np.zeros(N.MLP_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        N.check(self._L.fln_learned_gradients(self._h, _ptr(p), _ptr(X), _ptr(T), len(X),
+                                              float(quantile), _ptr(g), C.byref(loss)))
+        return loss.value, g
+
+
+def learned_options(**overrides) -> N.LearnedOptions:
+    o = N.LearnedOptions()
+    N.load().fln_learned_default_options(C.byref(o))
+    for k, v in overrides.items():
+        if not hasattr(o, k):
+            raise FlnError(1, f"unknown learned option {k}")
+        setattr(o, k, v)
+    return o
+
+
+class LearnedCriterion:
+    """The learned Barnes–Hut opening criterion (fln_learned)."""
+
+    def __init__(self, handle):
+        self._L = N.load()
+        self._h = handle
+
+    @classmethod
+    def train(cls, engine: Engine, xyz, loop_offsets, pairs, params: Optional[N.Params] = None,
+              options: Optional[N.LearnedOptions] = None, **option_overrides) -> "LearnedCriterion":
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        off = np.ascontiguousarray(loop_offsets, dtype=np.int64)
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        prm = params if params is not None else default_params()
+        opt = options if options is not None else learned_options(**option_overrides)
+        h = C.c_void_p()
+        L = N.load()
+        N.check(L.fln_learned_train(engine.handle, _ptr(xyz), _ptr(off), len(off) - 1, _ptr(pairs),
+                                    len(pairs), C.byref(prm), C.byref(opt), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_params(cls, params, s_min: float, log10_tau: float,
+                    min_candidates: int = 4) -> "LearnedCriterion":
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != N.MLP_PARAMS:
+            raise FlnError(1, f"expected {N.MLP_PARAMS} parameters")
+        h = C.c_void_p()
+        L = N.load()
+        N.check(L.fln_learned_create(_ptr(p), float(s_min), float(log10_tau), int(min_candidates),
+                                     C.byref(h)))
+        return cls(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(N.MLP_PARAMS, dtype=np.float32)
+        N.check(self._L.fln_learned_get(self._h, _ptr(p), None))
+        return p
+
+    def info(self) -> dict:
+        i = N.LearnedInfo()
+        N.check(self._L.fln_learned_get(self._h, None, C.byref(i)))
+        return i.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fln_learned_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
 
 def _method(m: str) -> int:
     if m == "directsum":

@@ -38,8 +38,10 @@
 #include <climits>
 #include <cmath>
 #include <numeric>
+#include <type_traits>
 
 #include "engine.hpp"
+#include "learned.cuh"
 
 namespace fln {
 
@@ -285,6 +287,15 @@ struct TravArgs {
   int2 *spill;                 // kSpill per warp
   unsigned long long *queue;   // batch queue head
   int32_t *status;             // nonzero on overflow
+  // Learned opening criterion (frag == nullptr: off).
+  LearnedCfg learned;
+  double beta0;
+  // Recording of training node pairs (rec == nullptr: off).
+  int4 *rec;
+  unsigned long long *rec_count;
+  int64_t rec_cap;
+  float rec_smin;
+  uint32_t rec_keep;           // keep a candidate when its hash is below this
 };
 
 // Fixed-point (2^-40) accumulation: integer adds commute, so per-pair sums do
@@ -450,15 +461,25 @@ __device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h
 // node pairs for at most `budget` steps; whatever is still on its stack then
 // is written out as new batches for the next round, so a heavy loop pair
 // spreads over many warps while light pairs finish in one go.
-__global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
+// kLearn: the learned opening criterion (A.learned); kRecord: sampling of
+// training node pairs (A.rec). The plain instantiation has neither.
+template <bool kLearn, bool kRecord>
+__device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
   __shared__ int2 s_leaf[kWarps][64];
+  __shared__ std::conditional_t<kLearn, MlpFrag, int> s_mlp;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + w;
   int2 *stack = s_stack[w];
   int2 *farq = s_far[w];
   int2 *leafq = s_leaf[w];
+  if constexpr (kLearn) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(A.learned.frag);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&s_mlp);
+    for (int x = threadIdx.x; x < (int)(sizeof(MlpFrag) / 4); x += blockDim.x) dst[x] = src[x];
+    __syncthreads();
+  }
   int2 *spill = A.spill + (size_t)gw * kSpill;
   double nfar = 0, nleaf = 0;
   for (;;) {
@@ -473,6 +494,8 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
     const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
     const NodeMom *M1 = A.mom + A.node_base[l1], *M2 = A.mom + A.node_base[l2];
     const double itolsq = A.itolsq[slot], eps = A.epssq;
+    // Threshold of the learned criterion: tau x (beta0 / beta)^4 in later passes.
+    const float log10_tau = A.learned.log10_tau + 2.f * (float)log10(A.beta0 * A.beta0 / itolsq);
     if (lane < cnt0) stack[lane] = A.in[b].pairs[lane];
     int top = cnt0, nspill = 0, nf = 0, nl = 0, steps = 0;
     bool overflow = false;
@@ -525,14 +548,18 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
       top -= cnt;
       int kind = 0;  // 0 none, 1 leaf, 2 far, 3 split
       int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
+      float sep = 0.f;
+      double dsq = 0.0;
       if (act) {
         const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
         const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
         const double rs = h1.r + h2.r;
+        dsq = dx * dx + dy * dy + dz * dz + eps;
+        sep = (float)(sqrt(dsq) / rs);
         if (leaf1 && leaf2) {
           kind = 1;
-        } else if (dx * dx + dy * dy + dz * dz + eps > rs * rs * itolsq + eps) {
+        } else if (dsq > rs * rs * itolsq + eps) {
           kind = 2;
         } else {
           kind = 3;
@@ -544,6 +571,36 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
             c0 = make_int2(h1.left, pr.y);
             c1 = make_int2(h1.right, pr.y);
           }
+        }
+      }
+      // Recording for training: opened pairs and far pairs near the threshold.
+      if (kRecord && act && kind != 1 && sep >= A.rec_smin && sep * sep <= 1.5625f * (float)itolsq) {
+        uint32_t hsh = (uint32_t)slot * 0x9E3779B1u ^ (uint32_t)pr.x * 0x85EBCA77u ^ (uint32_t)pr.y * 0xC2B2AE3Du;
+        hsh ^= hsh >> 15;
+        hsh *= 0x2C1B3C6Du;
+        hsh ^= hsh >> 12;
+        if (hsh < A.rec_keep) {
+          const unsigned long long at = atomicAdd(A.rec_count, 1ULL);
+          if ((int64_t)at < A.rec_cap) A.rec[at] = make_int4(slot, pr.x, pr.y, 0);
+        }
+      }
+      // Learned criterion: a pair the beta test opens but whose separation is
+      // at least s_min is accepted as far-field when the MLP predicts its
+      // error below tau; it then adds its Eq. 14 estimate to err like any
+      // far-field pair. The warp's candidates are evaluated at once, and only
+      // when there are at least min_cand (>= 1) of them.
+      if constexpr (kLearn) {
+        const bool cand = kind == 3 && sep >= A.learned.s_min;
+        if (__popc(__ballot_sync(0xffffffffu, cand)) >= A.learned.min_cand) {
+          float f[kMlpIn];
+          for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+          if (cand) {
+            const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+            const NodeMom &ma = M1[pr.x], &mb = M2[pr.y];
+            mlp_features(sep, (float)h1.r, (float)h2.r, dsq, ma.tn, mb.tn, ma.dn, mb.dn, ma.qn, mb.qn, f);
+          }
+          const float y = mlp_warp_predict(reinterpret_cast<const MlpFrag &>(s_mlp), f);
+          if (cand && y < log10_tau) kind = 2;
         }
       }
       const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
@@ -623,6 +680,11 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) {
     atomicAdd(A.counts + 1, nleaf);
   }
 }
+
+__global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { traverse<false, false>(A); }
+__global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true>(A); }
+// Four CTAs per SM, as the plain kernel gets with its natural register count.
+__global__ void __launch_bounds__(32 * kWarps, 4) bh_traverse_learned(TravArgs A) { traverse<true, false>(A); }
 
 // ------------------------------------------------------------------ split evaluation
 // Rounds with the evaluation taken out of the traversal: bh_classify walks
@@ -1279,6 +1341,83 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
   }
 }
 
+// Features and multipole value of recorded node pairs (thread per sample).
+__global__ void sample_features(const int64_t *node_base, const NodeHdr *hdr, const NodeMom *mom,
+                                const int32_t *slot_loops, const int4 *samples, int64_t n, double epssq, float *X,
+                                double *approx, float *sep_out, float *est_out, double err_scale) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int4 sm = samples[k];
+  const int l1 = slot_loops[2 * sm.x], l2 = slot_loops[2 * sm.x + 1];
+  const int64_t b1 = node_base[l1], b2 = node_base[l2];
+  const NodeHdr h1 = hdr[b1 + sm.y], h2 = hdr[b2 + sm.z];
+  const NodeMom &m1 = mom[b1 + sm.y], &m2 = mom[b2 + sm.z];
+  const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+  const double dsq = dx * dx + dy * dy + dz * dz + epssq;
+  const float sep = (float)(sqrt(dsq) / (h1.r + h2.r));
+  float f[kMlpIn];
+  mlp_features(sep, (float)h1.r, (float)h2.r, dsq, m1.tn, m2.tn, m1.dn, m2.dn, m1.qn, m2.qn, f);
+  for (int i = 0; i < kMlpIn; ++i) X[k * kMlpIn + i] = f[i];
+  double v = 0.0, e = 0.0;
+  far_eval(m1, m2, (float)dx, (float)dy, (float)dz, dsq, (float)h1.r, (float)h2.r, v, e);
+  approx[k] = v;
+  sep_out[k] = sep;
+  est_out[k] = (float)log10(e * err_scale + 1e-30);
+}
+
+// Segment range [lo, hi) of local node `node` of the curve-order tree over n
+// segments (the topology of curve_tree_topology).
+__device__ __forceinline__ void node_range(int64_t n, int32_t node, int64_t &lo, int64_t &hi) {
+  if (node >= n - 1) {
+    lo = node - (n - 1);
+    hi = lo + 1;
+    return;
+  }
+  const int64_t s = node + 1;
+  lo = 0;
+  hi = n;
+  for (int d = 0; d < 64; ++d) {
+    const int64_t m = lo + (hi - lo) / 2;
+    if (m == s) return;
+    if (s < m) hi = m;
+    else lo = m;
+  }
+}
+
+// One CTA per sample: the exact FP64 sum over the two nodes' segment ranges
+// (the leaf term seg_term_fp64) and the log10 error of the multipole value.
+__global__ void sample_exact(const double *xyz, const int64_t *off, const int32_t *slot_loops, const int4 *samples,
+                             const double *approx, int64_t n, int64_t max_terms, float *target, int32_t *valid) {
+  const int64_t k = blockIdx.x;
+  if (k >= n) return;
+  const int4 sm = samples[k];
+  const int la = slot_loops[2 * sm.x], lb = slot_loops[2 * sm.x + 1];
+  const int64_t oa = off[la], na = off[la + 1] - oa, ob = off[lb], nb = off[lb + 1] - ob;
+  int64_t a0, a1, b0, b1;
+  node_range(na, sm.y, a0, a1);
+  node_range(nb, sm.z, b0, b1);
+  if ((a1 - a0) * (b1 - b0) > max_terms) {
+    if (threadIdx.x == 0) valid[k] = 0;
+    return;
+  }
+  __shared__ double s_part[32];
+  const int64_t nbr = b1 - b0, terms = (a1 - a0) * nbr;
+  double acc = 0.0;
+  for (int64_t t = threadIdx.x; t < terms; t += blockDim.x) {
+    const int64_t i = a0 + t / nbr, j = b0 + t % nbr;
+    acc += seg_term_fp64(xyz, oa + i, oa + (i + 1 == na ? 0 : i + 1), ob + j, ob + (j + 1 == nb ? 0 : j + 1));
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+    target[k] = (float)log10(fabs(approx[k] - t) + 1e-14);
+    valid[k] = 1;
+  }
+}
+
 __global__ void scatter_kernel(const double *src, const int32_t *idx, int64_t n, double *dst) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) dst[idx[k]] = src[k];
@@ -1466,6 +1605,9 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   per_sm = std::max(per_sm, 1);
   const int grid = ctx.num_sms * per_sm;
   const int64_t nwarps = (int64_t)grid * kWarps;
+  int per_sm_l = 0;
+  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, bh_traverse_learned, 32 * kWarps, 0));
+  const int grid_l = ctx.num_sms * std::max(per_sm_l, 1);  // <= grid: the learned kernel uses more registers
   int per_sm_c = 0;
   FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, bh_classify, 32 * kWarps, 0));
   const int grid_c = ctx.num_sms * std::max(per_sm_c, 1);
@@ -1480,6 +1622,8 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
   const double b0 = prm.barnes_hut_init_beta;
   const int budget = 256;
+  if ((ctx.learned.frag || ctx.recording.rec) && prm.bh_schedule != 0)
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "The learned opening criterion runs with bh_schedule 0 only.");
   // Chunk lists of the split evaluation: a warp can write at most budget + 2
   // chunks per list after the soft limit stops new batches.
   const int64_t chunk_soft = int64_t(1) << FLN_CHUNK_SOFT_LOG2;
@@ -1491,7 +1635,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   }
   ctx.stats.bh_rounds = 0;
   // One Barnes–Hut pass over the slots in `active` with per-slot beta^2.
-  auto pass = [&](const std::vector<int32_t> &active, const std::vector<double> &itol_slots) {
+  auto pass = [&](const std::vector<int32_t> &active, const std::vector<double> &itol_slots, bool record) {
     const int64_t na = (int64_t)active.size();
     FLN_CUDA(cudaMemcpyAsync(d_active, active.data(), na * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     FLN_CUDA(cudaMemcpyAsync(d_itol, itol_slots.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1540,9 +1684,23 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         continue;
       }
       TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
-                 d_batch[1 - cur], cap, d_ctr + 1, budget, d_acc, d_acc_err, d_counts, d_spill, d_ctr, d_status};
-      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, grid));
-      bh_traverse<<<g, 32 * kWarps, 0, st>>>(A);
+                 d_batch[1 - cur], cap, d_ctr + 1, budget, d_acc, d_acc_err, d_counts, d_spill, d_ctr, d_status,
+                 ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
+      if (record) {
+        A.rec = ctx.recording.rec;
+        A.rec_count = ctx.recording.count;
+        A.rec_cap = ctx.recording.cap;
+        A.rec_smin = ctx.recording.s_min;
+        A.rec_keep = ctx.recording.keep;
+      }
+      const int gmax = (A.learned.frag && !A.rec) ? grid_l : grid;
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, gmax));
+      if (A.rec)
+        bh_traverse_record<<<g, 32 * kWarps, 0, st>>>(A);
+      else if (A.learned.frag)
+        bh_traverse_learned<<<g, 32 * kWarps, 0, st>>>(A);
+      else
+        bh_traverse<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
       ++launches;
       ++ctx.stats.bh_rounds;
@@ -1617,7 +1775,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   std::iota(all.begin(), all.end(), 0);
   std::vector<double> itol(np, b0 * b0);
   FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-  pass(all, itol);
+  pass(all, itol, ctx.recording.rec != nullptr);
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
   finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
   FLN_CUDA(cudaGetLastError());
@@ -1647,7 +1805,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   std::vector<double> far_leaf(2, 0.0);
   if (!retry_slots.empty()) {
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-    pass(retry_slots, itol);
+    pass(retry_slots, itol, false);
     FLN_CUDA(cudaEventRecord(ctx.ev3, st));
     finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
     FLN_CUDA(cudaGetLastError());
@@ -1682,7 +1840,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     if (up.empty()) break;
     ctx.stats.bh_escalated += (int64_t)up.size();
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-    pass(up, itol);
+    pass(up, itol, false);
     FLN_CUDA(cudaEventRecord(ctx.ev3, st));
     finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
     FLN_CUDA(cudaGetLastError());
@@ -1704,6 +1862,93 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
                                             std::to_string(maxdepth) + ").");
   return launches;
+}
+
+void learned_collect(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
+                     const std::vector<int32_t> &h_pairs, const fln_params &prm, float s_min, double keep,
+                     int64_t cap, int64_t max_terms, std::vector<float> &X, std::vector<float> &T,
+                     std::vector<float> &S, std::vector<float> &E, int64_t *recorded) {
+  X.clear();
+  T.clear();
+  S.clear();
+  E.clear();
+  if (recorded) *recorded = 0;
+  const int64_t np = (int64_t)h_pairs.size() / 2;
+  if (np == 0 || cap <= 0) return;
+  cudaStream_t st = ctx.stream;
+  int4 *d_rec = ctx.d_learn[0].as<int4>(cap);
+  unsigned long long *d_cnt = ctx.d_learn[1].as<unsigned long long>(1);
+  fln_params p = prm;
+  p.bh_tree = 0;
+  p.bh_schedule = 0;
+  double *d_lk = ctx.d_learn[2].as<double>(2 * np);
+  const LearnedCfg saved = ctx.learned;
+  unsigned long long cnt = 0;
+  // Records are written in traversal order, so a run that records more than
+  // cap would keep only its first (coarse) node pairs: such a run is repeated
+  // with a proportionally lower keep rate, which keeps the sample uniform.
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    FLN_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
+    ctx.learned = LearnedCfg{nullptr, 0.f, 0.f, 0};
+    ctx.recording.rec = d_rec;
+    ctx.recording.count = d_cnt;
+    ctx.recording.cap = cap;
+    ctx.recording.s_min = s_min;
+    ctx.recording.keep = (uint32_t)std::min(4294967295.0, std::max(0.0, keep) * 4294967296.0);
+    try {
+      barnes_hut_device(ctx, d_xyz, d_off, h_off, h_pairs, p, d_lk, d_lk + np, nullptr);
+    } catch (...) {
+      ctx.learned = saved;
+      ctx.recording = Recording{};
+      throw;
+    }
+    ctx.learned = saved;
+    ctx.recording = Recording{};
+    FLN_CUDA(cudaMemcpyAsync(&cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+    if ((int64_t)cnt <= cap) break;
+    keep *= 0.9 * (double)cap / (double)cnt;
+  }
+  if (recorded) *recorded = (int64_t)cnt;
+  const int64_t n = (int64_t)std::min<unsigned long long>(cnt, (unsigned long long)cap);
+  if (n == 0) return;
+  // The trees, node bases and slot loops of that call are still in place.
+  const int64_t *d_base = static_cast<const int64_t *>(ctx.d_bh[1].ptr);
+  const NodeHdr *d_hdr = static_cast<const NodeHdr *>(ctx.d_bh[9].ptr);
+  const NodeMom *d_mom = static_cast<const NodeMom *>(ctx.d_bh[10].ptr);
+  const int32_t *d_slots = static_cast<const int32_t *>(ctx.d_bh[11].ptr);
+  float *d_X = ctx.d_learn[3].as<float>(kMlpIn * n);
+  double *d_approx = ctx.d_learn[4].as<double>(n);
+  float *d_T = ctx.d_learn[5].as<float>(3 * n);
+  float *d_S = d_T + n, *d_E = d_T + 2 * n;
+  int32_t *d_valid = ctx.d_learn[6].as<int32_t>(n);
+  sample_features<<<(int)((n + 255) / 256), 256, 0, st>>>(d_base, d_hdr, d_mom, d_slots, d_rec, n, p.epssq, d_X,
+                                                           d_approx, d_S, d_E, p.error_est_scale);
+  FLN_CUDA(cudaGetLastError());
+  for (int64_t k0 = 0; k0 < n; k0 += (int64_t)1 << 30) {
+    const int64_t m = std::min<int64_t>(n - k0, (int64_t)1 << 30);
+    sample_exact<<<(int)m, 128, 0, st>>>(d_xyz, d_off, d_slots, d_rec + k0, d_approx + k0, m, max_terms, d_T + k0,
+                                         d_valid + k0);
+    FLN_CUDA(cudaGetLastError());
+  }
+  std::vector<float> hx(kMlpIn * n), ht(n), hs(n), he(n);
+  std::vector<int32_t> hv(n);
+  FLN_CUDA(cudaMemcpyAsync(hx.data(), d_X, hx.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(ht.data(), d_T, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(hs.data(), d_S, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(he.data(), d_E, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(hv.data(), d_valid, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaStreamSynchronize(st));
+  for (int64_t k = 0; k < n; ++k) {
+    if (!hv[k] || !std::isfinite(ht[k])) continue;
+    bool ok = true;
+    for (int i = 0; i < kMlpIn; ++i) ok = ok && std::isfinite(hx[kMlpIn * k + i]);
+    if (!ok) continue;
+    X.insert(X.end(), hx.begin() + kMlpIn * k, hx.begin() + kMlpIn * (k + 1));
+    T.push_back(ht[k]);
+    S.push_back(hs[k]);
+    E.push_back(he[k]);
+  }
 }
 
 }  // namespace fln

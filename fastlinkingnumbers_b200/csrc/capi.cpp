@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <numeric>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -38,6 +40,8 @@ Context::~Context() {
                     &d_near})
     b->release();
   for (auto &b : d_bh) b.release();
+  d_mlp.release();
+  for (auto &b : d_learn) b.release();
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (ev2) cudaEventDestroy(ev2);
@@ -159,6 +163,10 @@ struct fln_model {
 struct fln_certificate {
   Certificate c;
 };
+struct fln_learned {
+  std::vector<float> params;
+  fln_learned_info info{};
+};
 
 namespace fln {
 void set_last_error(const std::string &msg);
@@ -213,6 +221,26 @@ void compute_pairs_host(Context &ctx, const double *xyz, const int64_t *loop_off
   ctx.stats.ms_kernels = ms;
   ctx.stats.kernel_launches = launches;
   ctx.stats.ms_total = now_ms() - t0;
+}
+// Host loops and pairs -> the context's device buffers (checked).
+void upload_loops(Context &ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops, const int32_t *pairs,
+                  int64_t npairs, std::vector<int64_t> &h_off, std::vector<int32_t> &h_pairs, double **d_xyz,
+                  int64_t **d_off) {
+  if (!xyz || !loop_offsets || !pairs || nloops < 0 || npairs < 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+  FLN_CUDA(cudaSetDevice(ctx.device));
+  h_off.assign(loop_offsets, loop_offsets + nloops + 1);
+  h_pairs.assign(pairs, pairs + 2 * npairs);
+  check_inputs(h_off, nloops, h_pairs);
+  const int64_t nv = h_off[nloops];
+  *d_xyz = ctx.d_xyz.as<double>(3 * std::max<int64_t>(nv, 1));
+  *d_off = ctx.d_off.as<int64_t>(nloops + 1);
+  FLN_CUDA(cudaMemcpyAsync(*d_xyz, xyz, 3 * nv * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+  FLN_CUDA(cudaMemcpyAsync(*d_off, h_off.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+}
+
+double pinball(float y, float t, double q) {
+  const double e = (double)t - (double)y;
+  return e >= 0 ? q * e : (q - 1.0) * e;
 }
 }  // namespace
 
@@ -346,6 +374,202 @@ fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const d
     prm.precision = precision;
     const fln_params r = resolved(&prm);
     compute_pairs_host(*ctx->c, xyz.data(), off, 2, pr, 1, FLN_METHOD_DIRECTSUM, r, lk_out, nullptr, nullptr);
+  });
+}
+
+void fln_learned_default_options(fln_learned_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->s_min = 1.5;
+  o->sample_keep = 0.05;
+  o->max_samples = int64_t(1) << 20;
+  o->max_terms = int64_t(1) << 16;
+  o->epochs = 40;
+  o->batch = 4096;
+  o->learning_rate = 2e-3;
+  o->quantile = 0.9;
+  o->tau_quantile = 0.5;
+  o->val_fraction = 0.1;
+  o->min_candidates = 4;
+  o->seed = 1;
+}
+
+fln_status fln_learned_collect(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                               const int32_t *pairs, int64_t npairs, const fln_params *params, double s_min,
+                               double sample_keep, int64_t cap, int64_t max_terms, float *features_out,
+                               float *target_out, float *sep_out, float *est_out, int64_t *n_out) {
+  return guarded([&] {
+    if (!ctx || !n_out || cap < 0 || (cap > 0 && (!features_out || !target_out))) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    const fln_params prm = resolved(params);
+    std::vector<int64_t> h_off;
+    std::vector<int32_t> h_pairs;
+    double *d_xyz;
+    int64_t *d_off;
+    upload_loops(*ctx->c, xyz, loop_offsets, nloops, pairs, npairs, h_off, h_pairs, &d_xyz, &d_off);
+    std::vector<float> X, T, S, E;
+    int64_t recorded = 0;
+    learned_collect(*ctx->c, d_xyz, d_off, h_off, h_pairs, prm, (float)s_min, sample_keep, cap, max_terms, X, T, S,
+                    E, &recorded);
+    const int64_t n = (int64_t)T.size();
+    if (n > 0) {
+      std::memcpy(features_out, X.data(), X.size() * sizeof(float));
+      std::memcpy(target_out, T.data(), T.size() * sizeof(float));
+      if (sep_out) std::memcpy(sep_out, S.data(), S.size() * sizeof(float));
+      if (est_out) std::memcpy(est_out, E.data(), E.size() * sizeof(float));
+    }
+    *n_out = n;
+  });
+}
+
+fln_status fln_learned_train(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                             const int32_t *pairs, int64_t npairs, const fln_params *params,
+                             const fln_learned_options *options, fln_learned **out) {
+  return guarded([&] {
+    if (!ctx || !out) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    fln_learned_options o;
+    fln_learned_default_options(&o);
+    if (options) o = *options;
+    if (!(o.s_min > 0) || !(o.sample_keep > 0 && o.sample_keep <= 1) || o.max_samples <= 0 || o.max_terms <= 0 ||
+        o.epochs <= 0 || o.batch <= 0 || !(o.learning_rate > 0) || !(o.quantile > 0 && o.quantile < 1) ||
+        !(o.tau_quantile >= 0 && o.tau_quantile <= 1) || !(o.val_fraction >= 0 && o.val_fraction < 1))
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "learned options out of range");
+    const fln_params prm = resolved(params);
+    Context &c = *ctx->c;
+    std::vector<int64_t> h_off;
+    std::vector<int32_t> h_pairs;
+    double *d_xyz;
+    int64_t *d_off;
+    const double t0 = now_ms();
+    upload_loops(c, xyz, loop_offsets, nloops, pairs, npairs, h_off, h_pairs, &d_xyz, &d_off);
+    std::vector<float> X, T, S, E;
+    int64_t recorded = 0;
+    learned_collect(c, d_xyz, d_off, h_off, h_pairs, prm, (float)o.s_min, o.sample_keep, o.max_samples, o.max_terms,
+                    X, T, S, E, &recorded);
+    const double t1 = now_ms();
+    const int64_t n = (int64_t)T.size();
+    if (n < 256) throw Error(FLN_ERR_INVALID_ARGUMENT, "too few training samples (" + std::to_string(n) + ")");
+    // Threshold: the tau_quantile of the true errors of accepted far-field pairs.
+    const double b0 = prm.barnes_hut_init_beta;
+    std::vector<float> acc;
+    for (int64_t k = 0; k < n; ++k)
+      if (S[k] >= b0) acc.push_back(T[k]);
+    if (acc.empty()) throw Error(FLN_ERR_INVALID_ARGUMENT, "no recorded far-field pairs to set the threshold");
+    std::sort(acc.begin(), acc.end());
+    const double log10_tau = acc[std::min<size_t>(acc.size() - 1, (size_t)(o.tau_quantile * (acc.size() - 1) + 0.5))];
+    // Split, initialise (He normal), train.
+    std::mt19937_64 rng(o.seed);
+    std::vector<int32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::shuffle(idx.begin(), idx.end(), rng);
+    const int64_t nval = (int64_t)(o.val_fraction * n);
+    std::vector<int32_t> val(idx.begin(), idx.begin() + nval), train(idx.begin() + nval, idx.end());
+    std::vector<float> prm_mlp(FLN_MLP_PARAMS, 0.f);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    const int kIn = 8, kH = 64;
+    for (int k = 0; k < kIn * kH; ++k) prm_mlp[k] = nd(rng) * std::sqrt(2.f / kIn);
+    const int w2 = kIn * kH + kH, b2 = w2 + kH * kH, w3 = b2 + kH, b3 = w3 + kH;
+    for (int k = 0; k < kH * kH; ++k) prm_mlp[w2 + k] = nd(rng) * std::sqrt(2.f / kH);
+    for (int k = 0; k < kH; ++k) prm_mlp[w3 + k] = nd(rng) * std::sqrt(1.f / kH);
+    {
+      std::vector<float> tt;
+      for (int32_t r : train) tt.push_back(T[r]);
+      std::nth_element(tt.begin(), tt.begin() + tt.size() / 2, tt.end());
+      prm_mlp[b3] = tt[tt.size() / 2];
+    }
+    TrainOptions to;
+    to.epochs = o.epochs;
+    to.batch = o.batch;
+    to.lr = (float)o.learning_rate;
+    to.quantile = (float)o.quantile;
+    to.seed = o.seed;
+    const double train_loss = learned_train(c, X, T, train, to, prm_mlp);
+    double val_loss = 0, cover = 0;
+    if (nval > 0) {
+      std::vector<float> xv((size_t)kIn * nval), yv(nval);
+      for (int64_t k = 0; k < nval; ++k) std::memcpy(&xv[kIn * k], &X[(size_t)kIn * val[k]], kIn * sizeof(float));
+      learned_predict(c, prm_mlp.data(), xv.data(), nval, 0, yv.data());
+      for (int64_t k = 0; k < nval; ++k) {
+        val_loss += pinball(yv[k], T[val[k]], o.quantile);
+        cover += T[val[k]] <= yv[k] ? 1.0 : 0.0;
+      }
+      val_loss /= nval;
+      cover /= nval;
+    }
+    auto *m = new fln_learned;
+    m->params = std::move(prm_mlp);
+    fln_learned_info &inf = m->info;
+    inf.recorded = recorded;
+    inf.samples = n;
+    inf.train_samples = (int64_t)train.size();
+    inf.val_samples = nval;
+    inf.s_min = o.s_min;
+    inf.log10_tau = log10_tau;
+    inf.min_candidates = std::max(1, o.min_candidates);
+    inf.epochs = o.epochs;
+    inf.train_loss = train_loss;
+    inf.val_loss = val_loss;
+    inf.val_coverage = cover;
+    inf.ms_collect = t1 - t0;
+    inf.ms_train = now_ms() - t1;
+    *out = m;
+  });
+}
+
+fln_status fln_learned_create(const float *params, double s_min, double log10_tau, int32_t min_candidates,
+                              fln_learned **out) {
+  return guarded([&] {
+    if (!params || !out) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!(s_min > 0) || !std::isfinite(log10_tau)) throw Error(FLN_ERR_INVALID_ARGUMENT, "s_min or log10_tau");
+    for (int k = 0; k < FLN_MLP_PARAMS; ++k)
+      if (!std::isfinite(params[k])) throw Error(FLN_ERR_INVALID_ARGUMENT, "non-finite MLP parameter");
+    auto *m = new fln_learned;
+    m->params.assign(params, params + FLN_MLP_PARAMS);
+    m->info.s_min = s_min;
+    m->info.log10_tau = log10_tau;
+    m->info.min_candidates = std::max(1, min_candidates);
+    *out = m;
+  });
+}
+
+void fln_learned_destroy(fln_learned *m) { delete m; }
+
+fln_status fln_learned_get(const fln_learned *m, float *params_out, fln_learned_info *info_out) {
+  return guarded([&] {
+    if (!m) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL model");
+    if (params_out) std::memcpy(params_out, m->params.data(), FLN_MLP_PARAMS * sizeof(float));
+    if (info_out) *info_out = m->info;
+  });
+}
+
+fln_status fln_ctx_set_learned(fln_ctx *ctx, const fln_learned *m) {
+  return guarded([&] {
+    if (!ctx) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL context");
+    FLN_CUDA(cudaSetDevice(ctx->c->device));
+    if (!m) learned_enable(*ctx->c, nullptr, 0.f, 0.f, 0);
+    else
+      learned_enable(*ctx->c, m->params.data(), (float)m->info.s_min, (float)m->info.log10_tau,
+                     m->info.min_candidates);
+  });
+}
+
+fln_status fln_learned_predict(fln_ctx *ctx, const float *params, const float *features, int64_t n,
+                               int32_t use_mma, float *y_out) {
+  return guarded([&] {
+    if (!ctx || !params || (n > 0 && (!features || !y_out)) || n < 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    FLN_CUDA(cudaSetDevice(ctx->c->device));
+    learned_predict(*ctx->c, params, features, n, use_mma ? 1 : 0, y_out);
+  });
+}
+
+fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float *features,
+                                 const float *targets, int64_t n, double quantile, float *grad_out,
+                                 double *loss_out) {
+  return guarded([&] {
+    if (!ctx || !params || !features || !targets || !grad_out || n <= 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!(quantile > 0 && quantile < 1)) throw Error(FLN_ERR_INVALID_ARGUMENT, "quantile in (0, 1)");
+    FLN_CUDA(cudaSetDevice(ctx->c->device));
+    const double l = learned_gradients(*ctx->c, params, features, targets, n, (float)quantile, grad_out);
+    if (loss_out) *loss_out = l;
   });
 }
 

@@ -74,6 +74,26 @@ struct DirectPlan {
   double segment_pairs = 0;
 };
 
+// Learned opening criterion of the Barnes–Hut traversal (learned.cuh has the
+// weight layout; frag == nullptr: off).
+struct MlpFrag;
+struct LearnedCfg {
+  const MlpFrag *frag;  // device copy of the packed BF16 weights
+  float s_min;          // candidates: separation |dr| / (r1 + r2) at least this
+  float log10_tau;      // accept when the predicted log10 error is below this (at beta0)
+  int32_t min_cand;     // run the MLP only when a warp step has at least this many candidates
+};
+
+// Sampling of node pairs for training, during the first Barnes–Hut pass
+// (rec == nullptr: off). Pairs are (slot, node 1, node 2, 0).
+struct Recording {
+  int4 *rec = nullptr;
+  unsigned long long *count = nullptr;
+  int64_t cap = 0;
+  float s_min = 0.f;
+  uint32_t keep = 0;  // keep a candidate when its 32-bit hash is below this
+};
+
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -85,6 +105,10 @@ struct Context {
   DevBuf d_xyz, d_off, d_pairs, d_loops, d_items, d_partial, d_counter, d_lk, d_err, d_flags, d_near;
   DevBuf d_bh[24];
   HostBuf h_in, h_out;
+  // Learned criterion in use on this context, and training buffers.
+  DevBuf d_mlp, d_learn[8];
+  LearnedCfg learned{nullptr, 0.f, 0.f, 0};
+  Recording recording;
 
   explicit Context(int dev, void *user_stream);
   // Device time between two events recorded around launches on `stream`.
@@ -110,5 +134,41 @@ int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
 int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
                       const std::vector<int32_t> &h_pairs, const fln_params &prm, double *d_lk_out,
                       double *d_err_out, int32_t *d_flags_out);
+
+// Runs the Barnes–Hut stage (curve-order trees, beta0, learned criterion off)
+// while sampling node pairs with separation in [s_min, 1.25 beta0] (opened
+// pairs and far-field pairs near the threshold; a fraction `keep` of them by
+// a hash of (pair, node, node), lowered and rerun until at most `cap` are
+// recorded), then computes for each sample its features (learned.cuh) and
+// the log10 of the true far-field error: |multipole value - FP64 exact sum
+// over the two nodes' segment ranges| + 1e-14. Samples whose ranges hold more
+// than max_terms segment pairs are dropped. X gets 8 floats per sample, T the
+// target, S the separation, E log10 of the Eq. 14 estimate x err_scale (the
+// reference's error measure for the same pair).
+void learned_collect(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
+                     const std::vector<int32_t> &h_pairs, const fln_params &prm, float s_min, double keep,
+                     int64_t cap, int64_t max_terms, std::vector<float> &X, std::vector<float> &T,
+                     std::vector<float> &S, std::vector<float> &E, int64_t *recorded);
+
+// Training of the MLP on (X, T): pinball loss at quantile q, Adam, our own
+// kernels (learned.cu), on the rows idx_train. params holds kMlpParams FP32
+// values (initialised by the caller) and is updated; returns the mean loss of
+// the last epoch.
+struct TrainOptions {
+  int epochs = 40;
+  int batch = 4096;
+  float lr = 2e-3f;
+  float quantile = 0.9f;
+  uint64_t seed = 1;
+};
+double learned_train(Context &ctx, const std::vector<float> &X, const std::vector<float> &T,
+                     const std::vector<int32_t> &idx_train, const TrainOptions &opt, std::vector<float> &params);
+// FP32 (mma = 0) or BF16 warp-MMA (mma = 1, the traversal's path) predictions.
+void learned_predict(Context &ctx, const float *params, const float *X, int64_t n, int mma, float *Y);
+// Mean pinball loss and its gradient (d loss / d params) at params.
+double learned_gradients(Context &ctx, const float *params, const float *X, const float *T, int64_t n, float q,
+                         float *grad);
+// Packs params into the context's device weights and enables the criterion.
+void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand);
 
 }  // namespace fln

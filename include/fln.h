@@ -173,6 +173,94 @@ fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, const int64_t
                                               int32_t nloops, const int32_t *d_pairs, int64_t npairs,
                                               int32_t precision, double *d_lk_out, void *stream);
 
+/* ---- Learned opening criterion for Barnes–Hut. No counterpart in the
+ * reference, whose traversal opens a node pair exactly when
+ * |dr|^2 + eps^2 <= beta^2 (r1 + r2)^2 + eps^2 (compute_link.cpp:573-574, :608).
+ *
+ * A small MLP (8 -> 64 -> 64 -> 1, ReLU; BF16 weights, FP32 accumulation)
+ * predicts log10 of the true far-field error of a node pair from its
+ * separation s = |dr| / (r1 + r2), the radius ratio and the moment norms.
+ * With a model set on a context (fln_ctx_set_learned), the traversal accepts
+ * as far-field a pair the beta test would open when s >= s_min and the
+ * prediction is below log10_tau (tau scaled by (beta0 / beta)^4 in the retry
+ * and escalation passes); such a pair adds its Eq. 14 estimate to the error
+ * sum like any far-field pair, so the beta retry, the escalation, the margin
+ * check and the FP64 recompute keep their meaning and certificates keep
+ * their guarantees; only the set of evaluated node pairs changes.
+ * Barnes–Hut with bh_schedule 0 only (other schedules return
+ * FLN_ERR_INVALID_ARGUMENT while a model is set).
+ *
+ * Training (fln_learned_train): one Barnes–Hut run over the given loops
+ * records node pairs with s in [s_min, 1.25 beta0]; each gets its features
+ * and its true error against the FP64 exact sum over the two nodes' segment
+ * ranges; the MLP is fitted by our own forward/backward and Adam kernels
+ * under the pinball loss at `quantile` (an upper-quantile regression, so the
+ * prediction errs high); tau is the tau_quantile of the true errors of the
+ * recorded far-field pairs the beta test accepts (s in [beta0, 1.25 beta0]). */
+#define FLN_MLP_PARAMS 4801 /* W1[8][64], b1[64], W2[64][64], b2[64], w3[64], b3 (FP32) */
+
+typedef struct fln_learned_options {
+  double s_min;           /* 1.5 */
+  double sample_keep;     /* fraction of the candidate node pairs recorded: 0.05 */
+  int64_t max_samples;    /* 1 << 20 */
+  int64_t max_terms;      /* samples whose ranges hold more segment pairs are dropped: 1 << 16 */
+  int32_t epochs;         /* 40 */
+  int32_t batch;          /* 4096 */
+  double learning_rate;   /* 2e-3, cosine decay */
+  double quantile;        /* 0.9 */
+  double tau_quantile;    /* 0.5 */
+  double val_fraction;    /* held-out share of the samples: 0.1 */
+  int32_t min_candidates; /* the MLP runs for a warp step with at least this many candidates: 4 */
+  int32_t reserved0;
+  uint64_t seed;          /* 1 */
+  double reserved[4];
+} fln_learned_options;
+
+typedef struct fln_learned_info {
+  int64_t recorded;       /* node pairs recorded by the traversal */
+  int64_t samples;        /* of them with an exact target */
+  int64_t train_samples, val_samples;
+  double s_min, log10_tau;
+  int32_t min_candidates, epochs;
+  double train_loss, val_loss; /* pinball loss */
+  double val_coverage;    /* share of held-out samples whose true log10 error is <= the prediction */
+  double ms_collect, ms_train;
+  double reserved[4];
+} fln_learned_info;
+
+typedef struct fln_learned fln_learned;
+
+void fln_learned_default_options(fln_learned_options *o);
+fln_status fln_learned_train(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                             const int32_t *pairs, int64_t npairs, const fln_params *params,
+                             const fln_learned_options *options, fln_learned **out);
+/* A model from saved parameters (FLN_MLP_PARAMS floats). */
+fln_status fln_learned_create(const float *params, double s_min, double log10_tau, int32_t min_candidates,
+                              fln_learned **out);
+void fln_learned_destroy(fln_learned *m);
+/* Either output may be NULL. */
+fln_status fln_learned_get(const fln_learned *m, float *params_out, fln_learned_info *info_out);
+/* NULL turns the criterion off. The context keeps its own device copy. */
+fln_status fln_ctx_set_learned(fln_ctx *ctx, const fln_learned *m);
+/* Training samples as fln_learned_train records them: up to `cap` rows of
+ * features_out[8 * k], target_out[k] (log10 true error), sep_out[k] (the
+ * separation s) and est_out[k] (log10 of the Eq. 14 error estimate times
+ * error_est_scale, the reference's measure); sep_out and est_out may be NULL.
+ * *n_out gets the number written. */
+fln_status fln_learned_collect(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                               const int32_t *pairs, int64_t npairs, const fln_params *params, double s_min,
+                               double sample_keep, int64_t cap, int64_t max_terms, float *features_out,
+                               float *target_out, float *sep_out, float *est_out, int64_t *n_out);
+/* MLP outputs for n feature rows: FP32 (use_mma = 0) or the traversal's BF16
+ * warp-MMA path (use_mma = 1). */
+fln_status fln_learned_predict(fln_ctx *ctx, const float *params, const float *features, int64_t n,
+                               int32_t use_mma, float *y_out);
+/* Mean pinball loss at `quantile` over n rows and its gradient with respect
+ * to the FLN_MLP_PARAMS parameters (the training kernel's backward pass). */
+fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float *features,
+                                 const float *targets, int64_t n, double quantile, float *grad_out,
+                                 double *loss_out);
+
 /* One pair, host arrays (compute_link.h:62-64 and :86-87). */
 fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const double *xyz2,
                            int64_t n2, int32_t precision, double *lk_out);
