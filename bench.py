@@ -259,12 +259,18 @@ def run_ours(args, rank, world, local_rank):
     node_pairs = float(np.mean([s["bh_far_evals"] + s["bh_leaf_evals"] for s in st]))
     if args.method == "barneshut":
         achieved = BH_BYTES_PER_NODE_PAIR * node_pairs / (main_ms * 1e-3) / 1e9
+        traffic = args.traffic_bytes_per_node_pair * node_pairs if args.traffic_bytes_per_node_pair else None
         roof = {"bound": "hbm", "kernel": "bh_traverse", "achieved": achieved,
                 "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                "peak_source": peak_kind, "traffic": args.traffic_bytes,
+                "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": BH_BYTES_PER_NODE_PAIR * node_pairs,
                 "node_pairs_per_step": node_pairs, "ms_per_launch": main_ms,
-                "note": "algorithmic bytes = 2 x 184 B FP32 node record per evaluated node pair"}
+                "dram_gbs": traffic / (main_ms * 1e-3) / 1e9 if traffic else None,
+                "note": ("per step (all traversal rounds): algorithmic bytes = 2 x 184 B FP32 node "
+                         "record per evaluated node pair; traffic = DRAM read+write per node pair "
+                         "from the one-pass ncu capture in profiles/bh_traverse_polymer_10M_dram.md "
+                         "x node pairs; node records are mostly re-read from L1/L2, so the kernel "
+                         "is latency-bound, not HBM-bound")}
     else:
         roof = {"bound": "fp32-issue", "kernel": "direct_" + args.precision, "ms_per_launch": main_ms,
                 "segment_pairs_per_s": units / (main_ms * 1e-3)}
@@ -366,7 +372,8 @@ def main():
     ap.add_argument("--loop-steps", type=int, default=50000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
-    ap.add_argument("--traffic-bytes", type=float, default=None)
+    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=55.3,
+                    help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
     ap.add_argument("--learned-leg", type=int, default=1,
                     help="also train the learned opening criterion on another seed and time one step with it")
     args = ap.parse_args()

@@ -457,6 +457,24 @@ __device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h
   sum += kInvTwoPi * (double)atan2f(y, x) + (((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? (double)sg : 0.0);
 }
 
+// Software prefetch of node records (generic addresses; the records are
+// valid device memory). Bit 0: the next step's headers into L1; bit 1: the
+// moment records of queued far-field and leaf pairs into L1.
+// Traversal steps a warp takes on one batch per round before it hands the
+// rest of its stack on as new batches.
+#ifndef FLN_BH_BUDGET
+#define FLN_BH_BUDGET 256
+#endif
+#ifndef FLN_BH_PREFETCH
+#define FLN_BH_PREFETCH 3
+#endif
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.L1 [%0];" ::"l"(p)); }
+template <class T>
+__device__ __forceinline__ void prefetch_record(const T *p) {
+  prefetch_l1(p);
+  prefetch_l1(reinterpret_cast<const char *>(p) + sizeof(T) - 1);
+}
+
 // One warp per batch. The warp runs the two-tree traversal of its batch's
 // node pairs for at most `budget` steps; whatever is still on its stack then
 // is written out as new batches for the next round, so a heavy loop pair
@@ -629,9 +647,25 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
       if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
       if (kind == 1) leafq[nl + __popc(lm & ((1u << lane) - 1))] = pr;
+#if FLN_BH_PREFETCH & 2
+      if (kind == 1 || kind == 2) {
+        prefetch_record(M1 + pr.x);
+        prefetch_record(M2 + pr.y);
+      }
+#endif
       nf += __popc(fm);
       nl += __popc(lm);
       __syncwarp();
+#if FLN_BH_PREFETCH & 1
+      {  // the next step's headers, while the queued evaluations run
+        const int nxt = min(top, 32);
+        if (lane < nxt) {
+          const int2 p = stack[top - nxt + lane];
+          prefetch_record(H1 + p.x);
+          prefetch_record(H2 + p.y);
+        }
+      }
+#endif
       while (nf >= 32) {
         const int2 q = farq[nf - 32 + lane];
         const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
@@ -1621,7 +1655,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_slot_pair, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
   const double b0 = prm.barnes_hut_init_beta;
-  const int budget = 256;
+  const int budget = FLN_BH_BUDGET;
   if ((ctx.learned.frag || ctx.recording.rec) && prm.bh_schedule != 0)
     throw Error(FLN_ERR_INVALID_ARGUMENT, "The learned opening criterion runs with bh_schedule 0 only.");
   // Chunk lists of the split evaluation: a warp can write at most budget + 2
