@@ -457,16 +457,19 @@ __device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h
   sum += kInvTwoPi * (double)atan2f(y, x) + (((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? (double)sg : 0.0);
 }
 
-// Software prefetch of node records (generic addresses; the records are
-// valid device memory). Bit 0: the next step's headers into L1; bit 1: the
-// moment records of queued far-field and leaf pairs into L1.
 // Traversal steps a warp takes on one batch per round before it hands the
-// rest of its stack on as new batches.
+// rest of its stack on as new batches. Traversal time of the 14M-segment
+// polymer step on B200: 128 -> 208.2 ms, 256 -> 207.4 ms, 512 -> 222.5 ms,
+// 1024 -> 240.2 ms.
 #ifndef FLN_BH_BUDGET
 #define FLN_BH_BUDGET 256
 #endif
+// Software prefetch of node records (generic addresses; the records are
+// valid device memory). Bit 0: the next step's headers into L1; bit 1: the
+// moment records of queued far-field and leaf pairs into L1. Same step:
+// none 207.4 ms, bit 1 206.5 ms, bit 0 211.7 ms, both 212.2 ms.
 #ifndef FLN_BH_PREFETCH
-#define FLN_BH_PREFETCH 3
+#define FLN_BH_PREFETCH 2
 #endif
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.L1 [%0];" ::"l"(p)); }
 template <class T>
