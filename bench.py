@@ -57,6 +57,16 @@ def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000):
         cfg = {"workload": f"polymer loops: {loops} x {steps}-step closed Gaussian walks "
                            f"({loops * steps / 1e6:g}M segments), cube 400",
                "loops": loops, "steps_per_loop": steps}
+    elif name == "held_out_20M":
+        # Held-out evaluation set of the learned criterion: 1,000 walks of
+        # 20,000 steps at the polymer workload's density (cube 400 x 2^(1/3)).
+        off, xyz = W.polymer(seed=seed, n_loops=1000, n_steps=20000, cube=504.0)
+        cfg = {"workload": "held-out polymer: 1000 x 20000-step closed Gaussian walks (20M segments), "
+                           "cube 504", "loops": 1000, "steps_per_loop": 20000}
+    elif name == "mixed_batch":
+        off, xyz = W.mixed_batch(seed=seed)
+        cfg = {"workload": "mixed batch: 5000 loops, half (p,q) torus knots, half closed walks, sizes "
+                           "log-uniform in [16, 2^18] (134M segments), cube 600", "loops": 5000}
     elif name == "chain_mail":
         off, xyz = W.chain_mail(seed=seed)
         cfg = {"workload": "chain-mail sheet: 100 x 100 rings, 48-gons (480k segments)", "loops": 10000}
@@ -316,7 +326,13 @@ def run_ours(args, rank, world, local_rank):
         # workload family, on this workload: one step, against the plain one.
         from fastlinkingnumbers_b200 import LearnedCriterion
         t0 = time.perf_counter()
-        toff, txyz, tpairs, _ = make_workload(args.workload, args.seed + 1000, args.loops, args.loop_steps)
+        if args.workload == "held_out_20M":
+            from fastlinkingnumbers_b200 import workloads as W
+            toff, txyz, tpairs = W.walk_pairs(seed=args.seed + 1000)
+            trained_on = "20 pairs of interleaved 100,000-step closed walks (seed %d)" % (args.seed + 1000)
+        else:
+            toff, txyz, tpairs, _ = make_workload(args.workload, args.seed + 1000, args.loops, args.loop_steps)
+            trained_on = f"seed {args.seed + 1000} of the same workload family (held out)"
         model = LearnedCriterion.train(eng, txyz, toff, tpairs, params=prm)
         train_s = time.perf_counter() - t0
         eng.set_learned(model)
@@ -330,7 +346,7 @@ def run_ours(args, rank, world, local_rank):
         sl, llk = min(runs, key=lambda r: r[0]["ms_kernels"])
         info = model.info()
         result["learned_leg"] = {
-            "trained_on": f"seed {args.seed + 1000} of the same workload family (held out)",
+            "trained_on": trained_on,
             "train": {k: info[k] for k in ("recorded", "samples", "log10_tau", "s_min", "val_loss",
                                            "val_coverage", "ms_collect", "ms_train")},
             "train_wall_s_incl_workload": round(train_s, 2),
@@ -362,7 +378,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="polymer", choices=["polymer", "chain_mail", "ring_chain"])
+    ap.add_argument("--workload", default="polymer",
+                    choices=["polymer", "held_out_20M", "mixed_batch", "chain_mail", "ring_chain"])
     ap.add_argument("--method", default="barneshut", choices=["barneshut", "directsum"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--bh-tree", type=int, default=0)

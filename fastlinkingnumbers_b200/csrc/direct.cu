@@ -229,6 +229,12 @@ __device__ __forceinline__ void block_minmax7(float *lo, float *hi, float (*s_bo
   }
 }
 
+// Accumulation of a thread's terms over a tile: 0 = FP32, 1 = FP32 with
+// Kahan compensation, 2 = FP64.
+#ifndef FLN_MIXED_ACC
+#define FLN_MIXED_ACC 0
+#endif
+
 __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) {
   __shared__ float4 sq[kTile + 1];  // xyz relative to the tile origin; w = length of segment t
   __shared__ double s_red[kBlockSegs / 32];
@@ -310,6 +316,11 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
       float la = sqrtf(ax * ax + ay * ay + az * az), lb = sqrtf(bx_ * bx_ + by * by + bz * bz);
       float ab = ax * bx_ + ay * by + az * bz;
       float accf = 0.f;
+#if FLN_MIXED_ACC == 1
+      float comp = 0.f;  // Kahan compensation of accf
+#elif FLN_MIXED_ACC == 2
+      double accd = 0.0;
+#endif
       for (int k = 0; k < kt; ++k) {
         const float4 qn = sq[k + 1];
         const float cx = qn.x - r1x, cy = qn.y - r1y, cz = qn.z - r1z;
@@ -335,19 +346,36 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
           const float sdiv = div1 + div2;
           const float xp = div1 * div2 - det * det;
           const float yp = det * sdiv;
+          float term;
           if (sdiv > 0.f && fabsf(yp) < 0.25f * xp) {
-            accf += atan_small(__fdividef(yp, xp));  // principal branch, |angle| < 0.245
+            term = atan_small(__fdividef(yp, xp));  // principal branch, |angle| < 0.245
           } else {
-            accf += atan2f(yp, xp);
+            term = atan2f(yp, xp);
             if (sdiv < 0.f && det != 0.f) turns += (det > 0.f) ? 1 : -1;
           }
+#if FLN_MIXED_ACC == 1
+          const float y_ = term - comp;
+          const float t_ = accf + y_;
+          comp = (t_ - accf) - y_;
+          accf = t_;
+#elif FLN_MIXED_ACC == 2
+          accd += (double)term;
+#else
+          accf += term;
+#endif
         }
         q = qn;
         ax = dx; ay = dy; az = dz;
         bx_ = cx; by = cy; bz = cz;
         la = ld; lb = lc; ab = cd;
       }
+#if FLN_MIXED_ACC == 1
+      acc += (double)accf - (double)comp;
+#elif FLN_MIXED_ACC == 2
+      acc += accd;
+#else
       acc += (double)accf;
+#endif
     }
     const double v = active ? acc * kInvTwoPi + (double)turns + near_turns : 0.0;
     const double s = block_sum(v, s_red);

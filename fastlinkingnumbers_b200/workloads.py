@@ -122,11 +122,15 @@ def torus_knot(p, q, n, R=1.0, r=0.4, scale=1.0):
 
 
 def mixed_batch(seed=5, n_loops=5000, lo=16, hi=2 ** 18, cube=None):
-    """Torus knots and closed random walks, sizes log-uniform in [lo, hi]."""
+    """Torus knots and closed random walks, sizes log-uniform in [lo, hi].
+
+    The default cube side (35.1 x n_loops^(1/3), 600 for 5,000 loops) gives
+    35,717 potentially linked pairs for seed 5 (1.37e8 segments after
+    Discretize)."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(math.log(lo), math.log(hi), size=n_loops)).astype(np.int64)
     if cube is None:
-        cube = 60.0 * n_loops ** (1 / 3)
+        cube = 600.0 * (n_loops / 5000.0) ** (1 / 3)
     loops = []
     pq = [(p, q) for p in range(2, 10) for q in range(2, 10) if math.gcd(p, q) == 1 and p != q]
     for k in range(n_loops):
@@ -140,6 +144,23 @@ def mixed_batch(seed=5, n_loops=5000, lo=16, hi=2 ** 18, cube=None):
             pts = random_walk_loop(rng, max(n, 8), sigma=0.3)
         loops.append(pts + centre)
     return _pack(loops)
+
+
+def walk_pairs(seed=11, n_pairs=20, n_steps=100_000, offset=20.0):
+    """Training set of the learned criterion: n_pairs pairs of closed random
+    walks whose centres lie `offset` apart (so their trees interleave).
+    Returns (offsets, xyz, pairs)."""
+    rng = np.random.default_rng(seed)
+    loops, pairs = [], []
+    for k in range(n_pairs):
+        centre = rng.uniform(0.0, 1000.0, size=3)
+        d = rng.normal(size=3)
+        d *= offset / np.linalg.norm(d)
+        loops.append(random_walk_loop(rng, n_steps) + centre)
+        loops.append(random_walk_loop(rng, n_steps) + centre + d)
+        pairs.append((2 * k, 2 * k + 1))
+    off, xyz = _pack(loops)
+    return off, xyz, np.array(pairs, dtype=np.int32)
 
 
 def write_bcc(path, loops_or_packed, seg_type="PL"):

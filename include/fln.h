@@ -76,7 +76,7 @@ typedef struct fln_params {
   int32_t precision;            /* fln_precision; default FLN_PREC_MIXED */
   double fp64_margin;           /* recompute in FP64 when 0.5 - |lk - round(lk)| < this; default 0.25 */
   double near_factor;           /* mixed direct sum: a segment pair whose closest endpoint distance is
-                                   below near_factor * (longer segment length) is evaluated in FP64; 1.0 */
+                                   below near_factor * (longer segment length) is evaluated in FP64; 4.0 */
   int32_t bh_tree;              /* Barnes–Hut tree: 0 = curve-order tree (default), 1 = the reference's
                                    kd-median tree (ModifiedKdBVH.h:207-237) */
   int32_t bh_escalations;       /* after the reference's retry, a pair whose scaled error estimate is still
