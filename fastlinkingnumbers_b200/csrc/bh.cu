@@ -51,7 +51,19 @@ constexpr double kInvTwoPi = 0.15915494309189533576888376337251436;
 constexpr double kInvFourPi = 0.079577471545947667884441881686257181;
 constexpr double kInvRt3 = 0.57735026918962576450914878050195746;
 constexpr int kWarps = 4;          // warps per traversal CTA
-constexpr int kStack = 512;        // shared-memory stack entries per warp
+// Shared-memory stack entries per warp (> 128). 224 keeps a traversal CTA at
+// 11 KB of shared memory, so five CTAs fit a 64 KB carveout and leave the
+// rest of the SM's 256 KB to L1, which holds the node records the warps
+// re-read: 182.9 ms against 188.8 ms with 512 entries (14M-segment polymer
+// step, B200).
+#ifndef FLN_BH_STACK
+#define FLN_BH_STACK 224
+#endif
+// Preferred shared-memory carveout of the traversal kernel, percent.
+#ifndef FLN_BH_CARVEOUT
+#define FLN_BH_CARVEOUT 28
+#endif
+constexpr int kStack = FLN_BH_STACK;
 constexpr int kSpill = 8192;       // global spill entries per warp
 #ifndef FLN_CHUNK_SOFT_LOG2
 #define FLN_CHUNK_SOFT_LOG2 20  // chunks per list before a round stops taking batches
@@ -316,6 +328,13 @@ __device__ __forceinline__ float qrow(const float *q, int i, float rx, float ry,
   return q[4] * rx + q[5] * ry + q[2] * rz;
 }
 
+// Far-field scale factors in FP32 (1) or FP64 (0). FP32 drops the FP64
+// square root and divisions from the far-field path: 96 instead of 128
+// registers, five CTAs per SM instead of four, and 188.7 ms instead of
+// 206.4 ms for the traversal of the 14M-segment polymer step.
+#ifndef FLN_FAR_FP32_SCALE
+#define FLN_FAR_FP32_SCALE 1
+#endif
 // Far-field pair: monopole + Eq. 29 + Eq. 30 times 1/(4 pi |r|^3), and the
 // Eq. 14 estimate with the same factor (compute_link.cpp:608-627, :411-524).
 // Node 1 = u (moments m1 = "C" in the reference), node 2 = v ("D").
@@ -324,7 +343,15 @@ __device__ void far_eval(const NodeMom &m1, const NodeMom &m2, float rx, float r
   const float *C3 = m1.D, *D3 = m2.D;
   const float C1x = m1.t[0], C1y = m1.t[1], C1z = m1.t[2];
   const float D1x = m2.t[0], D1y = m2.t[1], D1z = m2.t[2];
+#if FLN_FAR_FP32_SCALE
+  // 1/|r|^2 and 1/(4 pi |r|^3) in FP32 (|r| > beta (r1 + r2), far from 0).
+  // Explicitly rounded operations: the error estimate (which decides the
+  // beta retry) must not depend on how a kernel's compile contracts them.
+  const float rinv = rsqrtf((float)dsq);
+  const float rdist2 = __fmul_rn(rinv, rinv);
+#else
   const float rdist2 = (float)(1.0 / dsq);
+#endif
   // monopole r . (c2 x c1)
   float res = rx * (D1y * C1z - D1z * C1y) + ry * (D1z * C1x - D1x * C1z) + rz * (D1x * C1y - D1y * C1x);
   // dipole (Eq. 29)
@@ -385,10 +412,15 @@ __device__ void far_eval(const NodeMom &m1, const NodeMom &m2, float rx, float r
   const float tfpq = 2.f * (Cr0 * wx + Cr1 * wy + Cr2 * wz);
   const float tf = tfpp + tfqq + tfpq;
   ho -= 1.5f * rdist2 * ((tqs + 2.f * tqt) + 5.f * rdist2 * tf);
+#if FLN_FAR_FP32_SCALE
+  const double mult = (double)__fmul_rn(__fmul_rn(rinv, rdist2), (float)kInvFourPi);
+#else
   const double mult = 1.0 / (dsq * sqrt(dsq)) * kInvFourPi;
+#endif
   sum += mult * ((double)res + (double)ho);
-  const float e = rdist2 * (m1.qn * (r1 * m2.tn + 3.f * m2.dn) + m2.qn * (r2 * m1.tn + 3.f * m1.dn));
-  err += mult * (double)e;
+  const float ea1 = __fmaf_rn(r1, m2.tn, __fmul_rn(3.f, m2.dn)), ea2 = __fmaf_rn(r2, m1.tn, __fmul_rn(3.f, m1.dn));
+  const float e = __fmul_rn(rdist2, __fmaf_rn(m1.qn, ea1, __fmul_rn(m2.qn, ea2)));
+  err = __fma_rn(mult, (double)e, err);
 }
 
 // Exact term of two segments in FP64 from their vertices (full turns).
@@ -476,6 +508,22 @@ template <class T>
 __device__ __forceinline__ void prefetch_record(const T *p) {
   prefetch_l1(p);
   prefetch_l1(reinterpret_cast<const char *>(p) + sizeof(T) - 1);
+}
+
+// stack[0, n) = stack[k, k + n), warp-wide, in passes of 32 that read before
+// they write: the lanes of a warp need not run the passes in step
+// (independent thread scheduling), so a lane ahead must not overwrite
+// entries that a lagging lane has yet to read. Out of line: it runs only
+// when a stack spills, and inlined it costs the traversal registers.
+__device__ __noinline__ void shift_down(int2 *stack, int k, int n, int lane) {
+  for (int xb = 0; xb < n; xb += 32) {
+    const int x = xb + lane;
+    int2 v = make_int2(0, 0);
+    if (x < n) v = stack[k + x];
+    __syncwarp();
+    if (x < n) stack[x] = v;
+    __syncwarp();
+  }
 }
 
 // One warp per batch. The warp runs the two-tree traversal of its batch's
@@ -634,8 +682,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         }
         for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
         __syncwarp();
-        // k >= kStack / 2 - 32 > 32, so no pass reads what an earlier write covered.
-        for (int x = lane; x < top - k; x += 32) stack[x] = stack[k + x];
+        shift_down(stack, k, top - k, lane);
         nspill += k;
         top -= k;
         __syncwarp();
@@ -718,7 +765,11 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
 }
 
+#ifdef FLN_BH_MIN_CTAS
+__global__ void __launch_bounds__(32 * kWarps, FLN_BH_MIN_CTAS) bh_traverse(TravArgs A) { traverse<false, false>(A); }
+#else
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { traverse<false, false>(A); }
+#endif
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true>(A); }
 // Four CTAs per SM, as the plain kernel gets with its natural register count.
 __global__ void __launch_bounds__(32 * kWarps, 4) bh_traverse_learned(TravArgs A) { traverse<true, false>(A); }
@@ -878,7 +929,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_classify(ClassifyArgs A) {
         }
         for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
         __syncwarp();
-        for (int x = lane; x < top - k; x += 32) stack[x] = stack[k + x];
+        shift_down(stack, k, top - k, lane);
         nspill += k;
         top -= k;
         __syncwarp();
@@ -1302,7 +1353,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
         }
         for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
         __syncwarp();
-        for (int x = lane; x < top - k; x += 32) stack[x] = stack[k + x];
+        shift_down(stack, k, top - k, lane);
         nspill += k;
         top -= k;
         __syncwarp();
@@ -1638,6 +1689,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   unsigned long long *d_acc_err = d_acc + np;
   unsigned long long *d_ctr = d_acc + 2 * np;  // [0] queue, [1] next-round count, [2] far chunks, [3] leaf chunks
   int per_sm = 0;
+  FLN_CUDA(cudaFuncSetAttribute(bh_traverse, cudaFuncAttributePreferredSharedMemoryCarveout, FLN_BH_CARVEOUT));
   FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_traverse, 32 * kWarps, 0));
   per_sm = std::max(per_sm, 1);
   const int grid = ctx.num_sms * per_sm;
