@@ -389,7 +389,7 @@ def main():
     ap.add_argument("--loop-steps", type=int, default=50000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
-    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=55.3,
+    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=67.0,
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
     ap.add_argument("--learned-leg", type=int, default=1,
                     help="also train the learned opening criterion on another seed and time one step with it")
