@@ -32,6 +32,7 @@
 // time, so the expensive branches run with full warps. Leaf-leaf pairs
 // closer than one segment length are evaluated in FP64 from the vertices.
 // Sums are FP64 per lane, reduced per pair in a fixed order.
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -213,8 +214,32 @@ __device__ void finish_record(const BuildNode &B, NodeHdr &H, NodeMom &M, bool l
   M.pad[0] = M.pad[1] = M.pad[2] = 0.f;
 }
 
-// Thread per leaf: initialise the leaf (compute_link.cpp:351-363) and walk
-// up; the second child to arrive at a parent builds it.
+// Leaf record of segment `seg` of a loop at vertex offset o with n segments
+// (compute_link.cpp:351-363): box, midpoint, tangent c, C_D = 0, and
+// C_Q,k = c_k c c^T / 12.
+__device__ void leaf_build(const double *xyz, int64_t o, int64_t n, int32_t seg, BuildNode &B) {
+  const int64_t v0 = o + seg, v1 = o + (seg + 1 == n ? 0 : seg + 1);
+  double p0[3], p1[3];
+  for (int a = 0; a < 3; ++a) {
+    p0[a] = xyz[3 * v0 + a];
+    p1[a] = xyz[3 * v1 + a];
+    B.lo[a] = fmin(p0[a], p1[a]);
+    B.hi[a] = fmax(p0[a], p1[a]);
+    B.mid[a] = 0.5 * p0[a] + 0.5 * p1[a];
+    B.t[a] = p1[a] - p0[a];
+  }
+  for (int a = 0; a < 9; ++a) B.D[a] = 0.0;
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int kk = 0; kk < 3; ++kk)
+    for (int e = 0; e < 6; ++e) B.Q[6 * kk + e] = ((1.0 / 12.0) * B.t[kk]) * (B.t[ii[e]] * B.t[jj[e]]);
+}
+
+// Thread per leaf: write the leaf's traversal record and walk up; the second
+// child to arrive at a parent builds it. Leaf build records are never
+// stored: a parent rebuilds a leaf child from its two vertices (48 B read
+// instead of a 312 B record written and read back). The arrival counter is
+// an acquire-release atomic, which orders the first child's record before
+// the second child's reads.
 __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t total) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
@@ -223,36 +248,24 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
   const int64_t o = A.off[l], n = A.off[l + 1] - o;
   const int64_t base = A.node_base[l];
   int32_t node = (int32_t)(n - 1 + (g - seg_start2[k]));
-  const int32_t seg = A.leaf_seg[base + node];
   {
+    const int32_t seg = A.leaf_seg[base + node];
     BuildNode B;
-    const int64_t v0 = o + seg, v1 = o + (seg + 1 == n ? 0 : seg + 1);
-    double p0[3], p1[3];
-    for (int a = 0; a < 3; ++a) {
-      p0[a] = A.xyz[3 * v0 + a];
-      p1[a] = A.xyz[3 * v1 + a];
-      B.lo[a] = fmin(p0[a], p1[a]);
-      B.hi[a] = fmax(p0[a], p1[a]);
-      B.mid[a] = 0.5 * p0[a] + 0.5 * p1[a];
-      B.t[a] = p1[a] - p0[a];
-    }
-    for (int a = 0; a < 9; ++a) B.D[a] = 0.0;
-    const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
-    for (int kk = 0; kk < 3; ++kk)
-      for (int e = 0; e < 6; ++e) B.Q[6 * kk + e] = ((1.0 / 12.0) * B.t[kk]) * (B.t[ii[e]] * B.t[jj[e]]);
-    A.bn[base + node] = B;
+    leaf_build(A.xyz, o, n, seg, B);
     finish_record(B, A.hdr[base + node], A.mom[base + node], true, seg, 0, 0);
   }
+  const int32_t first_leaf = (int32_t)(n - 1);
   for (int guard = 0; guard < 128; ++guard) {
     const int32_t par = A.parent[base + node];
     if (par < 0) break;
-    __threadfence();
-    if (atomicAdd(&A.arrive[base + par], 1) == 0) break;  // first arrival stops
-    __threadfence();
+    cuda::atomic_ref<int32_t, cuda::thread_scope_device> arrive(A.arrive[base + par]);
+    if (arrive.fetch_add(1, cuda::memory_order_acq_rel) == 0) break;  // first arrival stops
     const int32_t cl = A.children[2 * (base + par)], cr = A.children[2 * (base + par) + 1];
     BuildNode L, R;
-    load_cg(A.bn + base + cl, L);
-    load_cg(A.bn + base + cr, R);
+    if (cl >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cl], L);
+    else load_cg(A.bn + base + cl, L);
+    if (cr >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cr], R);
+    else load_cg(A.bn + base + cr, R);
     BuildNode P;
     for (int a = 0; a < 3; ++a) {
       P.lo[a] = fmin(L.lo[a], R.lo[a]);
