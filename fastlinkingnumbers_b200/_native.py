@@ -42,7 +42,7 @@ EXPORTED = [
     "fln_certificate_equals", "fln_certificate_export_diffs",
     "fln_learned_default_options", "fln_learned_train", "fln_learned_create", "fln_learned_destroy",
     "fln_learned_get", "fln_ctx_set_learned", "fln_learned_collect", "fln_learned_predict",
-    "fln_learned_gradients",
+    "fln_learned_gradients", "fln_model_prepare_device",
 ]
 
 MLP_PARAMS = 4801  # FLN_MLP_PARAMS
@@ -54,7 +54,7 @@ class Params(C.Structure):
         ("epssq", C.c_double), ("target_error", C.c_double), ("error_est_scale", C.c_double),
         ("precision", C.c_int32), ("fp64_margin", C.c_double), ("near_factor", C.c_double),
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
-        ("bh_schedule", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -143,6 +143,7 @@ def load():
     L.fln_model_num_points.restype = i64
     L.fln_model_get_curves.argtypes = [vp, P(i32), vp, vp]
     L.fln_model_prepare.argtypes = [vp, C.c_int, P(i32)]
+    L.fln_model_prepare_device.argtypes = [vp, vp, C.c_int, P(i32)]
     L.fln_model_prepared_sizes.argtypes = [vp, P(i64), P(i64)]
     L.fln_model_get_prepared.argtypes = [vp, vp, vp, vp]
     L.fln_certificate_compute.argtypes = [vp, vp, C.c_int, C.c_int, P(Params), P(vp)]

@@ -280,10 +280,14 @@ class Model:
     def num_curves(self) -> int:
         return self._L.fln_model_num_curves(self._h)
 
-    def Prepare(self, discretize: bool = True):
-        """PLS -> Discretize -> PLS. Returns (loop_offsets, xyz, pairs, rounds)."""
+    def Prepare(self, discretize: bool = True, engine: Optional["Engine"] = None):
+        """PLS -> Discretize -> PLS. Returns (loop_offsets, xyz, pairs, rounds).
+        With an engine the stages run on its GPU (same output bit for bit)."""
         r = C.c_int32()
-        N.check(self._L.fln_model_prepare(self._h, int(discretize), C.byref(r)))
+        if engine is None:
+            N.check(self._L.fln_model_prepare(self._h, int(discretize), C.byref(r)))
+        else:
+            N.check(self._L.fln_model_prepare_device(engine.handle, self._h, int(discretize), C.byref(r)))
         nv, npairs = C.c_int64(), C.c_int64()
         N.check(self._L.fln_model_prepared_sizes(self._h, C.byref(nv), C.byref(npairs)))
         off = np.zeros(self.num_curves() + 1, dtype=np.int64)

@@ -42,6 +42,7 @@ Context::~Context() {
   for (auto &b : d_bh) b.release();
   d_mlp.release();
   for (auto &b : d_learn) b.release();
+  for (auto &b : d_disc) b.release();
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (ev2) cudaEventDestroy(ev2);
@@ -170,7 +171,22 @@ struct fln_learned {
 
 namespace fln {
 void set_last_error(const std::string &msg);
+
+// prepare() with Discretize and both potential-link searches on the GPU.
+static void prepare_device(Context &ctx, Model &m, bool discretize_on) {
+  if (!discretize_on) {
+    prepare(m, false);
+    return;
+  }
+  discretize_device(ctx, m.curves, m.poly_offsets, m.poly_xyz, m.pairs, m.rounds);
+  // An open curve that reaches the linking-number stage is an error there
+  // (Curve::GetStartPoints, curve.cpp:126-128); one without pairs is not.
+  for (size_t p = 0; p < m.pairs.size(); ++p)
+    if (!m.curves[m.pairs[p]].closed)
+      throw Error(FLN_ERR_UNLOOPED, "Curve::GetStartPoints() does not support unlooped curves.");
+  m.prepared = true;
 }
+}  // namespace fln
 
 namespace {
 thread_local std::string g_last_error;
@@ -659,6 +675,16 @@ fln_status fln_model_prepare(fln_model *m, int discretize, int32_t *rounds_out) 
   });
 }
 
+fln_status fln_model_prepare_device(fln_ctx *ctx, fln_model *m, int discretize, int32_t *rounds_out) {
+  return guarded([&] {
+    if (!ctx || !m) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument");
+    FLN_CUDA(cudaSetDevice(ctx->c->device));
+    prepare_device(*ctx->c, m->m, discretize != 0);
+    m->prepared_disc = discretize != 0;
+    if (rounds_out) *rounds_out = m->m.rounds;
+  });
+}
+
 fln_status fln_model_prepared_sizes(const fln_model *m, int64_t *num_vertices, int64_t *num_pairs) {
   return guarded([&] {
     if (!m || !m->m.prepared) throw Error(FLN_ERR_INVALID_ARGUMENT, "model not prepared");
@@ -687,7 +713,9 @@ fln_status fln_certificate_compute(fln_ctx *ctx, const fln_model *model, int for
     auto *mm = const_cast<fln_model *>(model);  // the prepared polylines are a cache
     const double t0 = now_ms();
     if (!mm->m.prepared || mm->prepared_disc != (discretize != 0)) {
-      prepare(mm->m, discretize != 0);
+      FLN_CUDA(cudaSetDevice(ctx->c->device));
+      if (prm.host_prepare) prepare(mm->m, discretize != 0);
+      else prepare_device(*ctx->c, mm->m, discretize != 0);
       mm->prepared_disc = discretize != 0;
     }
     const double t1 = now_ms();

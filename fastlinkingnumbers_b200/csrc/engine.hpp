@@ -107,6 +107,8 @@ struct Context {
   HostBuf h_in, h_out;
   // Learned criterion in use on this context, and training buffers.
   DevBuf d_mlp, d_learn[8];
+  // Device Discretize (discretize.cu).
+  DevBuf d_disc[34];
   LearnedCfg learned{nullptr, 0.f, 0.f, 0};
   Recording recording;
 
@@ -168,6 +170,13 @@ void learned_predict(Context &ctx, const float *params, const float *X, int64_t 
 // Mean pinball loss and its gradient (d loss / d params) at params.
 double learned_gradients(Context &ctx, const float *params, const float *X, const float *T, int64_t n, float q,
                          float *grad);
+// Discretize (discretize.cpp:103-281) and the potential-link searches before
+// and after it, on the GPU: the same closed polylines (CSR offsets, xyz) and
+// sorted unique pairs (i < j) as the host path, bit for bit; rounds = the
+// refinement rounds run. Throws Error on the reference's failure conditions.
+void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::vector<int64_t> &offsets,
+                       std::vector<double> &xyz, std::vector<int32_t> &pairs, int32_t &rounds);
+
 // Packs params into the context's device weights and enables the criterion.
 void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand);
 

@@ -5,7 +5,18 @@
 // evaluation order: src/curve.cpp:20-43 (bases), :156-184 (get_point),
 // :197-277 (compute_box_1d), :293-324 (get_segment_bounding_box). This file
 // is compiled with -ffp-contract=off so no product or sum is fused.
+//
+// The raw piece functions (seg_point, seg_box) are also compiled for the GPU
+// (discretize.cu, built with --fmad=false; CUDA's division and square root
+// are correctly rounded), so the device Discretize reproduces these boxes
+// bit for bit.
 #pragma once
+
+#ifdef __CUDACC__
+#define FLN_HD __host__ __device__
+#else
+#define FLN_HD
+#endif
 
 #include <cmath>
 #include <cstdint>
@@ -31,8 +42,8 @@ inline bool overlaps(const Box3 &a, const Box3 &b) {
   return a.lo[0] <= b.hi[0] && a.lo[1] <= b.hi[1] && a.lo[2] <= b.hi[2] && b.lo[0] <= a.hi[0] &&
          b.lo[1] <= a.hi[1] && b.lo[2] <= a.hi[2];
 }
-inline double min_of(double a, double b) { return (b < a) ? b : a; }
-inline double max_of(double a, double b) { return (a < b) ? b : a; }
+FLN_HD inline double min_of(double a, double b) { return (b < a) ? b : a; }
+FLN_HD inline double max_of(double a, double b) { return (a < b) ? b : a; }
 inline void grow(Box3 &a, const Box3 &b) {
   for (int d = 0; d < 3; ++d) {
     a.lo[d] = min_of(a.lo[d], b.lo[d]);
@@ -46,6 +57,109 @@ inline double diag_length(const Box3 &b) {
 
 enum SegKind : int { kBSpline = 0, kCatmullRom = 1, kBezier = 2, kPolyline = 3 };
 
+// Cubic coefficients (t^3, t^2, t, 1) of one coordinate of a spline segment
+// given its four control values; the monomial forms of curve.cpp:205-233.
+FLN_HD inline void seg_cubic(int k, double q1, double q2, double q3, double q4, double c[4]) {
+  if (k == kBSpline) {
+    c[0] = -(1.0 / 6.0) * q1 + 0.5 * q2 - 0.5 * q3 + (1.0 / 6.0) * q4;
+    c[1] = 0.5 * q1 - q2 + 0.5 * q3;
+    c[2] = -0.5 * q1 + 0.5 * q3;
+    c[3] = (1.0 / 6.0) * q1 + (2.0 / 3.0) * q2 + (1.0 / 6.0) * q3;
+  } else if (k == kCatmullRom) {
+    c[0] = -0.5 * q1 + 1.5 * q2 - 1.5 * q3 + 0.5 * q4;
+    c[1] = 1.0 * q1 - 2.5 * q2 + 2.0 * q3 - 0.5 * q4;
+    c[2] = -0.5 * q1 + 0.5 * q3;
+    c[3] = 1.0 * q2;
+  } else {
+    c[0] = -1.0 * q1 + 3.0 * q2 - 3.0 * q3 + 1.0 * q4;
+    c[1] = 3.0 * q1 - 6.0 * q2 + 3.0 * q3;
+    c[2] = -3.0 * q1 + 3.0 * q2;
+    c[3] = 1.0 * q1;
+  }
+}
+
+// Point on segment `seg` of a curve with n control points q (3 doubles
+// each) at parameter t (Horner bases of curve.cpp:20-43).
+FLN_HD inline void seg_point(int kind, const double *q, int64_t n, int64_t seg, double t, double out[3]) {
+  if (kind == kPolyline) {
+    const double *s = q + 3 * seg, *e = q + 3 * ((seg + 1) % n);
+    const double u = 1.0 - t;
+    for (int d = 0; d < 3; ++d) out[d] = u * s[d] + t * e[d];
+    return;
+  }
+  double B[4];
+  if (kind == kBSpline) {
+    B[0] = ((-(1.0 / 6) * t + (1.0 / 2)) * t - (1.0 / 2)) * t + (1.0 / 6);
+    B[1] = ((1.0 / 2) * t - 1.0) * (t * t) + (2.0 / 3);
+    B[2] = ((-(1.0 / 2) * t + (1.0 / 2)) * t + (1.0 / 2)) * t + (1.0 / 6);
+    B[3] = (1.0 / 6) * (t * t) * t;
+  } else if (kind == kCatmullRom) {
+    B[0] = ((-0.5 * t + 1.0) * t - 0.5) * t;
+    B[1] = (1.5 * t - 2.5) * (t * t) + 1.0;
+    B[2] = ((-1.5 * t + 2.0) * t + 0.5) * t;
+    B[3] = (0.5 * t - 0.5) * (t * t);
+  } else {
+    B[0] = ((-1.0 * t + 3.0) * t - 3.0) * t + 1.0;
+    B[1] = ((3.0 * t - 6.0) * t + 3.0) * t;
+    B[2] = (-3.0 * t + 3.0) * (t * t);
+    B[3] = 1.0 * t * t * t;
+  }
+  const double *a = q + 3 * seg, *b = q + 3 * ((seg + 1) % n), *c = q + 3 * ((seg + 2) % n),
+               *dd = q + 3 * ((seg + 3) % n);
+  for (int d = 0; d < 3; ++d) out[d] = ((B[0] * a[d] + B[1] * b[d]) + B[2] * c[d]) + B[3] * dd[d];
+}
+
+// Extent of one cubic coordinate over [t0, t1]: the endpoint values and any
+// interior stationary point (roots of the derivative by the stable
+// quadratic formula), as curve.cpp:234-276 evaluates them.
+FLN_HD inline double cubic_at(const double c[4], double s) { return ((c[0] * s + c[1]) * s + c[2]) * s + c[3]; }
+FLN_HD inline void cubic_take(const double c[4], double s, double t0, double t1, double &lo, double &hi) {
+  if (s >= t0 && s <= t1) {
+    const double v = cubic_at(c, s);
+    lo = min_of(lo, v);
+    hi = max_of(hi, v);
+  }
+}
+FLN_HD inline void cubic_extent(const double c[4], double t0, double t1, double &lo, double &hi) {
+  lo = cubic_at(c, t0);
+  hi = cubic_at(c, t1);
+  if (hi < lo) {
+    const double tmp = lo;
+    lo = hi;
+    hi = tmp;
+  }
+  const double disc = 4 * c[1] * c[1] - 12 * c[2] * c[0];
+  if (disc == 0) {
+    cubic_take(c, -2 * c[1] / (6 * c[0]), t0, t1, lo, hi);
+    return;
+  }
+  const double rad = (c[1] >= 0) ? -2 * c[1] - sqrt(disc) : -2 * c[1] + sqrt(disc);
+  cubic_take(c, rad / (6 * c[0]), t0, t1, lo, hi);
+  cubic_take(c, 2 * c[2] / rad, t0, t1, lo, hi);
+}
+
+// Closed box of piece [t0, t1] of segment `seg` (curve.cpp:293-324).
+FLN_HD inline void seg_box(int kind, const double *q, int64_t n, int64_t seg, double t0, double t1, double lo[3],
+                           double hi[3]) {
+  if (kind == kPolyline) {
+    double a[3], e[3];
+    seg_point(kind, q, n, seg, t0, a);
+    seg_point(kind, q, n, seg, t1, e);
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = min_of(a[d], e[d]);
+      hi[d] = max_of(a[d], e[d]);
+    }
+    return;
+  }
+  const double *p0 = q + 3 * seg, *p1 = q + 3 * ((seg + 1) % n), *p2 = q + 3 * ((seg + 2) % n),
+               *p3 = q + 3 * ((seg + 3) % n);
+  for (int d = 0; d < 3; ++d) {
+    double c[4];
+    seg_cubic(kind, p0[d], p1[d], p2[d], p3[d], c);
+    cubic_extent(c, t0, t1, lo[d], hi[d]);
+  }
+}
+
 // A curve of the model: control points (closed or open) and a segment kind.
 struct CurveData {
   std::vector<Vec3> q;
@@ -58,106 +172,16 @@ struct CurveData {
     return kind == kPolyline ? n - 1 : n - 3;
   }
 
-  // Cubic coefficients (t^3, t^2, t, 1) of one coordinate of a spline segment
-  // given its four control values; the monomial forms of curve.cpp:205-233.
-  static void cubic(SegKind k, double q1, double q2, double q3, double q4, double c[4]) {
-    if (k == kBSpline) {
-      c[0] = -(1.0 / 6.0) * q1 + 0.5 * q2 - 0.5 * q3 + (1.0 / 6.0) * q4;
-      c[1] = 0.5 * q1 - q2 + 0.5 * q3;
-      c[2] = -0.5 * q1 + 0.5 * q3;
-      c[3] = (1.0 / 6.0) * q1 + (2.0 / 3.0) * q2 + (1.0 / 6.0) * q3;
-    } else if (k == kCatmullRom) {
-      c[0] = -0.5 * q1 + 1.5 * q2 - 1.5 * q3 + 0.5 * q4;
-      c[1] = 1.0 * q1 - 2.5 * q2 + 2.0 * q3 - 0.5 * q4;
-      c[2] = -0.5 * q1 + 0.5 * q3;
-      c[3] = 1.0 * q2;
-    } else {
-      c[0] = -1.0 * q1 + 3.0 * q2 - 3.0 * q3 + 1.0 * q4;
-      c[1] = 3.0 * q1 - 6.0 * q2 + 3.0 * q3;
-      c[2] = -3.0 * q1 + 3.0 * q2;
-      c[3] = 1.0 * q1;
-    }
-  }
-
-  // Point on segment `seg` at parameter t (Horner bases of curve.cpp:20-43).
+  // Point on segment `seg` at parameter t.
   Vec3 at(int seg, double t) const {
-    const size_t n = q.size();
-    if (kind == kPolyline) {
-      const Vec3 &s = q[seg], &e = q[(seg + 1) % n];
-      const double u = 1.0 - t;
-      return {u * s.x + t * e.x, u * s.y + t * e.y, u * s.z + t * e.z};
-    }
-    double B[4];
-    if (kind == kBSpline) {
-      B[0] = ((-(1.0 / 6) * t + (1.0 / 2)) * t - (1.0 / 2)) * t + (1.0 / 6);
-      B[1] = ((1.0 / 2) * t - 1.0) * (t * t) + (2.0 / 3);
-      B[2] = ((-(1.0 / 2) * t + (1.0 / 2)) * t + (1.0 / 2)) * t + (1.0 / 6);
-      B[3] = (1.0 / 6) * (t * t) * t;
-    } else if (kind == kCatmullRom) {
-      B[0] = ((-0.5 * t + 1.0) * t - 0.5) * t;
-      B[1] = (1.5 * t - 2.5) * (t * t) + 1.0;
-      B[2] = ((-1.5 * t + 2.0) * t + 0.5) * t;
-      B[3] = (0.5 * t - 0.5) * (t * t);
-    } else {
-      B[0] = ((-1.0 * t + 3.0) * t - 3.0) * t + 1.0;
-      B[1] = ((3.0 * t - 6.0) * t + 3.0) * t;
-      B[2] = (-3.0 * t + 3.0) * (t * t);
-      B[3] = 1.0 * t * t * t;
-    }
-    const Vec3 &a = q[seg], &b = q[(seg + 1) % n], &c = q[(seg + 2) % n], &d = q[(seg + 3) % n];
-    return {((B[0] * a.x + B[1] * b.x) + B[2] * c.x) + B[3] * d.x,
-            ((B[0] * a.y + B[1] * b.y) + B[2] * c.y) + B[3] * d.y,
-            ((B[0] * a.z + B[1] * b.z) + B[2] * c.z) + B[3] * d.z};
-  }
-
-  // Extent of one cubic coordinate over [t0, t1]: the endpoint values and any
-  // interior stationary point (roots of the derivative by the stable
-  // quadratic formula), as curve.cpp:234-276 evaluates them.
-  static void extent(const double c[4], double t0, double t1, double &lo, double &hi) {
-    auto ev = [&](double s) { return ((c[0] * s + c[1]) * s + c[2]) * s + c[3]; };
-    lo = ev(t0);
-    hi = ev(t1);
-    if (hi < lo) {
-      const double tmp = lo;
-      lo = hi;
-      hi = tmp;
-    }
-    auto take = [&](double s) {
-      if (s >= t0 && s <= t1) {
-        const double v = ev(s);
-        lo = min_of(lo, v);
-        hi = max_of(hi, v);
-      }
-    };
-    const double disc = 4 * c[1] * c[1] - 12 * c[2] * c[0];
-    if (disc == 0) {
-      take(-2 * c[1] / (6 * c[0]));
-      return;
-    }
-    const double rad = (c[1] >= 0) ? -2 * c[1] - std::sqrt(disc) : -2 * c[1] + std::sqrt(disc);
-    take(rad / (6 * c[0]));
-    take(2 * c[2] / rad);
+    double o[3];
+    seg_point(kind, &q[0].x, (int64_t)q.size(), seg, t, o);
+    return {o[0], o[1], o[2]};
   }
 
   Box3 piece_box(int seg, double t0 = 0.0, double t1 = 1.0) const {
     Box3 b;
-    if (kind == kPolyline) {
-      const Vec3 a = at(seg, t0), e = at(seg, t1);
-      const double av[3] = {a.x, a.y, a.z}, ev[3] = {e.x, e.y, e.z};
-      for (int d = 0; d < 3; ++d) {
-        b.lo[d] = min_of(av[d], ev[d]);
-        b.hi[d] = max_of(av[d], ev[d]);
-      }
-      return b;
-    }
-    const size_t n = q.size();
-    const Vec3 &p0 = q[seg], &p1 = q[(seg + 1) % n], &p2 = q[(seg + 2) % n], &p3 = q[(seg + 3) % n];
-    const double v[3][4] = {{p0.x, p1.x, p2.x, p3.x}, {p0.y, p1.y, p2.y, p3.y}, {p0.z, p1.z, p2.z, p3.z}};
-    for (int d = 0; d < 3; ++d) {
-      double c[4];
-      cubic(kind, v[d][0], v[d][1], v[d][2], v[d][3], c);
-      extent(c, t0, t1, b.lo[d], b.hi[d]);
-    }
+    seg_box(kind, &q[0].x, (int64_t)q.size(), seg, t0, t1, b.lo, b.hi);
     return b;
   }
 

@@ -86,7 +86,9 @@ typedef struct fln_params {
   int32_t bh_schedule;          /* 0 = budgeted rounds, evaluation inside the traversal (default);
                                    1 = one persistent launch with a device work queue;
                                    2 = budgeted rounds, evaluation in separate streaming kernels */
-  int32_t reserved[3];
+  int32_t host_prepare;         /* fln_certificate_compute: 0 = Discretize and the potential-link searches
+                                   on the context's GPU (default), 1 = on the host; same output bit for bit */
+  int32_t reserved[2];
 } fln_params;
 
 /* Statistics of the last computation on a context. */
@@ -288,6 +290,10 @@ fln_status fln_model_get_curves(const fln_model *m, int32_t *type_out, int32_t *
  * discretized closed polylines and the sorted unique (i < j) pairs into
  * buffers owned by the model (read them with fln_model_get_prepared). */
 fln_status fln_model_prepare(fln_model *m, int discretize, int32_t *rounds_out);
+/* The same stages with Discretize and both potential-link searches on the
+ * context's GPU: bit-identical polylines, pairs and round count (the piece
+ * boxes use the host's arithmetic with no fused multiply-add). */
+fln_status fln_model_prepare_device(fln_ctx *ctx, fln_model *m, int discretize, int32_t *rounds_out);
 fln_status fln_model_prepared_sizes(const fln_model *m, int64_t *num_vertices, int64_t *num_pairs);
 fln_status fln_model_get_prepared(const fln_model *m, int64_t *loop_offsets_out, double *xyz_out,
                                   int32_t *pairs_out);
