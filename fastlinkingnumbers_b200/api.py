@@ -290,9 +290,9 @@ class Model:
             N.check(self._L.fln_model_prepare_device(engine.handle, self._h, int(discretize), C.byref(r)))
         nv, npairs = C.c_int64(), C.c_int64()
         N.check(self._L.fln_model_prepared_sizes(self._h, C.byref(nv), C.byref(npairs)))
-        off = np.zeros(self.num_curves() + 1, dtype=np.int64)
-        xyz = np.zeros((max(nv.value, 1), 3))
-        pairs = np.zeros((max(npairs.value, 1), 2), dtype=np.int32)
+        off = np.empty(self.num_curves() + 1, dtype=np.int64)
+        xyz = np.empty((max(nv.value, 1), 3))
+        pairs = np.empty((max(npairs.value, 1), 2), dtype=np.int32)
         N.check(self._L.fln_model_get_prepared(self._h, _ptr(off), _ptr(xyz), _ptr(pairs)))
         return off, xyz[:nv.value], pairs[:npairs.value], r.value
 

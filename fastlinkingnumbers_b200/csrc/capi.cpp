@@ -47,7 +47,81 @@ Context::~Context() {
   if (ev1) cudaEventDestroy(ev1);
   if (ev2) cudaEventDestroy(ev2);
   if (ev3) cudaEventDestroy(ev3);
+  for (cudaEvent_t e : ev_stage)
+    if (e) cudaEventDestroy(e);
   if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+void parallel_memcpy(void *dst, const void *src, size_t bytes) {
+  const size_t kBlock = size_t(1) << 20;
+  const int64_t nb = (int64_t)((bytes + kBlock - 1) / kBlock);
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < nb; ++b) {
+    const size_t o = (size_t)b * kBlock;
+    std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, std::min(kBlock, bytes - o));
+  }
+}
+
+static bool is_pinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+static constexpr size_t kStage = size_t(64) << 20;
+
+static void stage_setup(Context &ctx) {
+  ctx.h_in.need(kStage);
+  ctx.h_out.need(kStage);
+  for (cudaEvent_t &e : ctx.ev_stage)
+    if (!e) FLN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+void copy_h2d(Context &ctx, void *d_dst, const void *h_src, size_t bytes) {
+  if (bytes == 0) return;
+  if (bytes <= kStage / 4 || is_pinned(h_src)) {
+    FLN_CUDA(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, ctx.stream));
+    FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+    return;
+  }
+  stage_setup(ctx);
+  void *stage[2] = {ctx.h_in.ptr, ctx.h_out.ptr};
+  for (size_t o = 0, k = 0; o < bytes; o += kStage, ++k) {
+    const size_t len = std::min(kStage, bytes - o);
+    FLN_CUDA(cudaEventSynchronize(ctx.ev_stage[k & 1]));  // the copy that last used this buffer is done
+    parallel_memcpy(stage[k & 1], static_cast<const char *>(h_src) + o, len);
+    FLN_CUDA(cudaMemcpyAsync(static_cast<char *>(d_dst) + o, stage[k & 1], len, cudaMemcpyHostToDevice, ctx.stream));
+    FLN_CUDA(cudaEventRecord(ctx.ev_stage[k & 1], ctx.stream));
+  }
+  FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void copy_d2h(Context &ctx, void *h_dst, const void *d_src, size_t bytes) {
+  if (bytes == 0) return;
+  if (bytes <= kStage / 4 || is_pinned(h_dst)) {
+    FLN_CUDA(cudaMemcpyAsync(h_dst, d_src, bytes, cudaMemcpyDeviceToHost, ctx.stream));
+    FLN_CUDA(cudaStreamSynchronize(ctx.stream));
+    return;
+  }
+  stage_setup(ctx);
+  void *stage[2] = {ctx.h_in.ptr, ctx.h_out.ptr};
+  const size_t nchunks = (bytes + kStage - 1) / kStage;
+  for (size_t k = 0; k <= nchunks; ++k) {
+    if (k < nchunks) {
+      const size_t o = k * kStage, len = std::min(kStage, bytes - o);
+      FLN_CUDA(cudaMemcpyAsync(stage[k & 1], static_cast<const char *>(d_src) + o, len, cudaMemcpyDeviceToHost,
+                               ctx.stream));
+      FLN_CUDA(cudaEventRecord(ctx.ev_stage[k & 1], ctx.stream));
+    }
+    if (k > 0) {
+      const size_t j = k - 1, o = j * kStage, len = std::min(kStage, bytes - o);
+      FLN_CUDA(cudaEventSynchronize(ctx.ev_stage[j & 1]));
+      parallel_memcpy(static_cast<char *>(h_dst) + o, stage[j & 1], len);
+    }
+  }
 }
 
 // Scatters src[k] into dst[idx[k]] for the FP64 recompute (defined in bh.cu).
@@ -223,7 +297,7 @@ void compute_pairs_host(Context &ctx, const double *xyz, const int64_t *loop_off
   double *d_err = ctx.d_err.as<double>(std::max<int64_t>(npairs, 1));
   int32_t *d_flags = ctx.d_flags.as<int32_t>(std::max<int64_t>(npairs, 1));
   FLN_CUDA(cudaEventRecord(ctx.ev0, ctx.stream));
-  FLN_CUDA(cudaMemcpyAsync(d_xyz, xyz, 3 * nv * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+  copy_h2d(ctx, d_xyz, xyz, 3 * nv * sizeof(double));
   FLN_CUDA(cudaMemcpyAsync(d_off, h_off.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
   const int launches = run_pairs(ctx, d_xyz, d_off, h_off, h_pairs, method, prm, d_lk, d_err, d_flags);
   FLN_CUDA(cudaEventRecord(ctx.ev1, ctx.stream));
@@ -699,7 +773,7 @@ fln_status fln_model_get_prepared(const fln_model *m, int64_t *loop_offsets_out,
     if (!m || !m->m.prepared) throw Error(FLN_ERR_INVALID_ARGUMENT, "model not prepared");
     if (loop_offsets_out)
       std::memcpy(loop_offsets_out, m->m.poly_offsets.data(), m->m.poly_offsets.size() * sizeof(int64_t));
-    if (xyz_out) std::memcpy(xyz_out, m->m.poly_xyz.data(), m->m.poly_xyz.size() * sizeof(double));
+    if (xyz_out) parallel_memcpy(xyz_out, m->m.poly_xyz.data(), m->m.poly_xyz.size() * sizeof(double));
     if (pairs_out) std::memcpy(pairs_out, m->m.pairs.data(), m->m.pairs.size() * sizeof(int32_t));
   });
 }

@@ -498,7 +498,7 @@ std::vector<Box3> boxes_to_host(Context &ctx, const double *d_box, int nc) {
 }  // namespace
 
 void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::vector<int64_t> &offsets,
-                       std::vector<double> &xyz, std::vector<int32_t> &pairs_out, int32_t &rounds) {
+                       DoubleArray &xyz, std::vector<int32_t> &pairs_out, int32_t &rounds) {
   const int nc = (int)curves.size();
   cudaStream_t st = ctx.stream;
   DevBuf *B = ctx.d_disc;
@@ -510,24 +510,21 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
     seg_off[c + 1] = seg_off[c] + std::max(curves[c].segments(), 0);
     kind[c] = curves[c].kind;
   }
-  std::vector<double> cp(3 * (size_t)std::max<int64_t>(cp_off[nc], 1));
-  for (int c = 0; c < nc; ++c)
-    for (size_t k = 0; k < curves[c].q.size(); ++k) {
-      const Vec3 &v = curves[c].q[k];
-      double *o = &cp[3 * (cp_off[c] + (int64_t)k)];
-      o[0] = v.x;
-      o[1] = v.y;
-      o[2] = v.z;
+  DoubleArray cp(3 * (size_t)std::max<int64_t>(cp_off[nc], 1));
+  const int64_t nseg = seg_off[nc];
+  DoubleArray norms((size_t)std::max<int64_t>(nseg, 1));
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int c = 0; c < nc; ++c) {
+    if (!curves[c].q.empty()) std::memcpy(&cp[3 * cp_off[c]], &curves[c].q[0].x, curves[c].q.size() * sizeof(Vec3));
+    for (int s = 0; s < curves[c].segments(); ++s) {
+      const Vec3 &p = curves[c].q[s];
+      norms[seg_off[c] + s] = std::sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
     }
+  }
   // Input sanity (discretize.cpp:126-160): mean |control point| over the
   // segment-indexed points, summed in the host's order.
   double norm_sum = 0;
-  const int64_t nseg = seg_off[nc];
-  for (int c = 0; c < nc; ++c)
-    for (int s = 0; s < curves[c].segments(); ++s) {
-      const Vec3 &p = curves[c].q[s];
-      norm_sum += std::sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
-    }
+  for (int64_t k = 0; k < nseg; ++k) norm_sum += norms[k];
   const double avg = norm_sum / ((double)nseg * 1.73205080757);
   const double thresh = std::numeric_limits<double>::epsilon() * avg;
   if (nseg > INT32_MAX) throw Error(FLN_ERR_OUT_OF_MEMORY, "Discretize: more than 2^31 segments");
@@ -536,7 +533,7 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
   int64_t *d_cpoff = buf<int64_t>(B[1], nc + 1);
   int32_t *d_kind = buf<int32_t>(B[2], nc);
   int64_t *d_segoff = buf<int64_t>(B[3], nc + 1);
-  FLN_CUDA(cudaMemcpyAsync(d_cp, cp.data(), cp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  copy_h2d(ctx, d_cp, cp.data(), 3 * cp_off[nc] * sizeof(double));
   FLN_CUDA(cudaMemcpyAsync(d_cpoff, cp_off.data(), (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_kind, kind.data(), std::max(nc, 1) * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_segoff, seg_off.data(), (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
@@ -750,9 +747,9 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
                                                                             d_pstart, d_out, d_xyz);
   }
   FLN_CUDA(cudaGetLastError());
+  FLN_CUDA(cudaStreamSynchronize(st));
   xyz.resize(3 * nv);
-  if (nv > 0)
-    FLN_CUDA(cudaMemcpyAsync(xyz.data(), d_xyz, 3 * nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+  copy_d2h(ctx, xyz.data(), d_xyz, 3 * nv * sizeof(double));
   // Potential pairs of the polylines.
   double *d_box = buf<double>(B[27], 6 * (int64_t)nc);
   if (nc > 0) polyline_boxes<<<nc, 256, 0, st>>>(d_xyz, d_out, d_box);

@@ -104,7 +104,8 @@ struct Context {
   // Device buffers.
   DevBuf d_xyz, d_off, d_pairs, d_loops, d_items, d_partial, d_counter, d_lk, d_err, d_flags, d_near;
   DevBuf d_bh[24];
-  HostBuf h_in, h_out;
+  HostBuf h_in, h_out;  // pinned staging of copy_h2d / copy_d2h
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   // Learned criterion in use on this context, and training buffers.
   DevBuf d_mlp, d_learn[8];
   // Device Discretize (discretize.cu).
@@ -175,7 +176,16 @@ double learned_gradients(Context &ctx, const float *params, const float *X, cons
 // sorted unique pairs (i < j) as the host path, bit for bit; rounds = the
 // refinement rounds run. Throws Error on the reference's failure conditions.
 void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::vector<int64_t> &offsets,
-                       std::vector<double> &xyz, std::vector<int32_t> &pairs, int32_t &rounds);
+                       DoubleArray &xyz, std::vector<int32_t> &pairs, int32_t &rounds);
+
+// Host<->device copies on ctx.stream that return when the data has arrived.
+// Pinned host memory is copied directly; pageable memory goes in 64 MB
+// chunks through two pinned buffers, the host side by all threads (a single
+// pageable DMA copy runs at a few GB/s, slower still into fresh pages).
+void copy_h2d(Context &ctx, void *d_dst, const void *h_src, size_t bytes);
+void copy_d2h(Context &ctx, void *h_dst, const void *d_src, size_t bytes);
+// memcpy by all host threads.
+void parallel_memcpy(void *dst, const void *src, size_t bytes);
 
 // Packs params into the context's device weights and enables the criterion.
 void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand);

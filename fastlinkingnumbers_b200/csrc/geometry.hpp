@@ -28,6 +28,7 @@ namespace fln {
 struct Vec3 {
   double x, y, z;
 };
+static_assert(sizeof(Vec3) == 3 * sizeof(double), "Vec3 is three packed doubles");
 inline Vec3 operator-(const Vec3 &a, const Vec3 &b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 
 // Closed-interval box; the default is empty (intersects nothing), like

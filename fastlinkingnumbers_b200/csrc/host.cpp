@@ -242,7 +242,7 @@ int64_t dual_walk(const RangeTree &A, const std::vector<Box3> &ba, std::atomic<u
 }  // namespace
 
 void discretize(const std::vector<CurveData> &curves, const std::vector<std::vector<int>> &links,
-                std::vector<int64_t> &offsets, std::vector<double> &xyz, int32_t &rounds) {
+                std::vector<int64_t> &offsets, DoubleArray &xyz, int32_t &rounds) {
   const int nc = (int)curves.size();
   std::vector<std::vector<Piece>> live(nc), done(nc);
   std::vector<std::vector<Box3>> lbox(nc);

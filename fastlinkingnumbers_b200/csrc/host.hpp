@@ -3,6 +3,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -20,12 +22,35 @@ struct Error : std::runtime_error {
   Error(fln_status s, const std::string &m) : std::runtime_error(m), status(s) {}
 };
 
+// An allocator that default-initialises: resize() leaves doubles unwritten,
+// so a large array's pages are first touched by whoever fills it (all
+// threads of a parallel copy) instead of being zeroed by one thread.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) noexcept {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+using DoubleArray = std::vector<double, NoInitAlloc<double>>;
+
 struct Model {
   std::vector<CurveData> curves;
   // Prepared (discretized) closed polylines, CSR over loops, and the sorted
   // unique potential pairs (i < j) of those polylines.
   std::vector<int64_t> poly_offsets;
-  std::vector<double> poly_xyz;
+  DoubleArray poly_xyz;
   std::vector<int32_t> pairs;  // 2 per pair
   int32_t rounds = 0;
   bool prepared = false;
@@ -41,7 +66,7 @@ std::vector<std::pair<int, int>> box_pairs(const std::vector<Box3> &boxes);
 // discretize.cpp:103-281; `links[i]` lists every curve whose box meets curve
 // i's (both directions). Throws Error on the reference's failure conditions.
 void discretize(const std::vector<CurveData> &curves, const std::vector<std::vector<int>> &links,
-                std::vector<int64_t> &offsets, std::vector<double> &xyz, int32_t &rounds);
+                std::vector<int64_t> &offsets, DoubleArray &xyz, int32_t &rounds);
 
 // PLS -> Discretize -> PLS (lnc.cpp:61-83 and :367-381).
 void prepare(Model &m, bool discretize_on);
