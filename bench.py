@@ -50,7 +50,7 @@ def _peaks():
         return PEAKS_FALLBACK, "fallback"
 
 
-def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000):
+def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000, engine=None):
     from fastlinkingnumbers_b200 import Model, workloads as W
     if name == "polymer":
         off, xyz = W.polymer(seed=seed, n_loops=loops, n_steps=steps)
@@ -79,8 +79,9 @@ def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000):
                 "l2": "inputs and per-step trees larger than L2 (no flush needed)"})
     m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
     t0 = time.perf_counter()
-    poff, pxyz, pairs, rounds = m.Prepare(True)
-    cfg["host_prepare_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+    poff, pxyz, pairs, rounds = m.Prepare(True, engine=engine)
+    cfg["prepare_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+    cfg["prepare_on"] = "host" if engine is None else "gpu"
     cfg["discretize_rounds"] = int(rounds)
     cfg["segments_after_discretize"] = int(poff[-1])
     cfg["pairs"] = int(len(pairs))
@@ -192,9 +193,9 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank, args.loops, args.loop_steps)
     stream = torch.cuda.current_stream()
     eng = Engine(local_rank, stream.cuda_stream)
+    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank, args.loops, args.loop_steps, engine=eng)
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
                            bh_tree=args.bh_tree, bh_schedule=args.bh_schedule)
     d_xyz = torch.from_numpy(pxyz).cuda()
@@ -331,7 +332,7 @@ def run_ours(args, rank, world, local_rank):
             toff, txyz, tpairs = W.walk_pairs(seed=args.seed + 1000)
             trained_on = "20 pairs of interleaved 100,000-step closed walks (seed %d)" % (args.seed + 1000)
         else:
-            toff, txyz, tpairs, _ = make_workload(args.workload, args.seed + 1000, args.loops, args.loop_steps)
+            toff, txyz, tpairs, _ = make_workload(args.workload, args.seed + 1000, args.loops, args.loop_steps, engine=eng)
             trained_on = f"seed {args.seed + 1000} of the same workload family (held out)"
         model = LearnedCriterion.train(eng, txyz, toff, tpairs, params=prm)
         train_s = time.perf_counter() - t0

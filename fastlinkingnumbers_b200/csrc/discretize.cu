@@ -545,6 +545,13 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
     return Pieces{buf<int32_t>(b[0], n), buf<int32_t>(b[1], n), buf<double>(b[2], n), buf<double>(b[3], n),
                   buf<uint8_t>(b[4], n)};
   };
+  // Per-piece arrays with room for growth: refinement usually adds a few
+  // tens of percent, and each reallocation would cost a device-wide free.
+  const int64_t reserve = nseg + nseg / 2 + 1024;
+  pieces(0, reserve);
+  pieces(1, reserve);
+  for (int k : {14, 15}) buf<int32_t>(B[k], reserve);
+  buf<uint8_t>(B[28], reserve);
   int cur = 0;
   int64_t n = nseg;
   Pieces P = pieces(cur, n);
