@@ -198,6 +198,12 @@ def run_ours(args, rank, world, local_rank):
     poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank, args.loops, args.loop_steps, engine=eng)
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
                            bh_tree=args.bh_tree, bh_schedule=args.bh_schedule)
+    tune = None
+    if args.autotune and args.method == "barneshut":
+        # Round budget only: the same node pairs, so results change only in the
+        # rounding of partial sums (beta stays the reference's 2). Tuned on a
+        # seeded sample of the pairs, untimed.
+        prm, tune = eng.autotune(pxyz, poff, pairs, tune_beta=False, sample_pairs=2048, params=prm)
     d_xyz = torch.from_numpy(pxyz).cuda()
     d_off = torch.from_numpy(poff).cuda()
     d_pairs = torch.from_numpy(pairs).cuda()
@@ -294,6 +300,7 @@ def run_ours(args, rank, world, local_rank):
                          "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median",
                          "schedule": ["rounds, fused evaluation", "persistent queue", "rounds, split evaluation"][args.bh_schedule]},
         "certificate_ms": ms,
+        "autotune": tune,
         "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(pxyz.nbytes + poff.nbytes + pairs.nbytes),
                 "d2h_bytes_per_step": int(npairs * (8 + 8 + 4))},
@@ -392,6 +399,8 @@ def main():
     ap.add_argument("--direct-sample", type=int, default=64)
     ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=67.0,
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="tune the Barnes-Hut round budget on a sample of the pairs before timing")
     ap.add_argument("--learned-leg", type=int, default=1,
                     help="also train the learned opening criterion on another seed and time one step with it")
     args = ap.parse_args()

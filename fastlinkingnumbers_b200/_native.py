@@ -42,8 +42,19 @@ EXPORTED = [
     "fln_certificate_equals", "fln_certificate_export_diffs",
     "fln_learned_default_options", "fln_learned_train", "fln_learned_create", "fln_learned_destroy",
     "fln_learned_get", "fln_ctx_set_learned", "fln_learned_collect", "fln_learned_predict",
-    "fln_learned_gradients", "fln_model_prepare_device",
+    "fln_learned_gradients", "fln_model_prepare_device", "fln_autotune",
 ]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("best_ms", C.c_double), ("default_ms", C.c_double), ("trials", C.c_int32),
+        ("sample_pairs", C.c_int32), ("best_budget", C.c_int32), ("reserved0", C.c_int32),
+        ("best_beta", C.c_double), ("reserved", C.c_double * 3),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 MLP_PARAMS = 4801  # FLN_MLP_PARAMS
 
@@ -54,7 +65,8 @@ class Params(C.Structure):
         ("epssq", C.c_double), ("target_error", C.c_double), ("error_est_scale", C.c_double),
         ("precision", C.c_int32), ("fp64_margin", C.c_double), ("near_factor", C.c_double),
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
-        ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("bh_budget", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
 
@@ -144,6 +156,7 @@ def load():
     L.fln_model_get_curves.argtypes = [vp, P(i32), vp, vp]
     L.fln_model_prepare.argtypes = [vp, C.c_int, P(i32)]
     L.fln_model_prepare_device.argtypes = [vp, vp, C.c_int, P(i32)]
+    L.fln_autotune.argtypes = [vp, vp, vp, i32, vp, i64, P(Params), i32, i64, P(Params), P(TuneResult)]
     L.fln_model_prepared_sizes.argtypes = [vp, P(i64), P(i64)]
     L.fln_model_get_prepared.argtypes = [vp, vp, vp, vp]
     L.fln_certificate_compute.argtypes = [vp, vp, C.c_int, C.c_int, P(Params), P(vp)]

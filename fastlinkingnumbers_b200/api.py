@@ -89,6 +89,21 @@ class Engine:
                                         C.byref(out)))
         return out.value
 
+    def autotune(self, xyz, loop_offsets, pairs, tune_beta: bool = False, sample_pairs: int = 0,
+                 params: Optional[N.Params] = None, **overrides):
+        """Fastest Barnes-Hut settings on a seeded sample of the pairs:
+        (tuned Params, result dict). Beta is tuned only if tune_beta."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        off = np.ascontiguousarray(loop_offsets, dtype=np.int64)
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        prm = params if params is not None else default_params(**overrides)
+        out = N.Params()
+        res = N.TuneResult()
+        N.check(self._L.fln_autotune(self._h, _ptr(xyz), _ptr(off), len(off) - 1, _ptr(pairs), len(pairs),
+                                     C.byref(prm), int(tune_beta), int(sample_pairs), C.byref(out),
+                                     C.byref(res)))
+        return out, res.as_dict()
+
     # ---- learned opening criterion (no counterpart in the reference)
     def set_learned(self, model: Optional["LearnedCriterion"]):
         """Uses `model` for the Barnes–Hut opening decisions of this engine (None: off)."""

@@ -1723,7 +1723,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_slot_pair, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
   const double b0 = prm.barnes_hut_init_beta;
-  const int budget = FLN_BH_BUDGET;
+  const int budget = prm.bh_budget > 0 ? prm.bh_budget : FLN_BH_BUDGET;
   if ((ctx.learned.frag || ctx.recording.rec) && prm.bh_schedule != 0)
     throw Error(FLN_ERR_INVALID_ARGUMENT, "The learned opening criterion runs with bh_schedule 0 only.");
   // Chunk lists of the split evaluation: a warp can write at most budget + 2

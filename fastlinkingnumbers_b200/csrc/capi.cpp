@@ -221,6 +221,8 @@ static fln_params resolved(const fln_params *p) {
     throw Error(FLN_ERR_INVALID_ARGUMENT, "Barnes-Hut beta must be positive");
   if (r.bh_escalations < 0 || r.bh_escalations > 8) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_escalations in [0, 8]");
   if (r.bh_schedule < 0 || r.bh_schedule > 2) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_schedule in [0, 2]");
+  if (r.bh_budget != 0 && (r.bh_budget < 16 || r.bh_budget > 4096))
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_budget 0 or in [16, 4096]");
   return r;
 }
 
@@ -660,6 +662,86 @@ fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float 
     FLN_CUDA(cudaSetDevice(ctx->c->device));
     const double l = learned_gradients(*ctx->c, params, features, targets, n, (float)quantile, grad_out);
     if (loss_out) *loss_out = l;
+  });
+}
+
+fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                        const int32_t *pairs, int64_t npairs, const fln_params *params, int32_t tune_beta,
+                        int64_t sample_pairs, fln_params *out, fln_tune_result *result) {
+  return guarded([&] {
+    if (!ctx || !out || npairs <= 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument or no pairs");
+    const fln_params base = resolved(params);
+    Context &c = *ctx->c;
+    std::vector<int64_t> h_off;
+    std::vector<int32_t> h_all;
+    double *d_xyz;
+    int64_t *d_off;
+    upload_loops(c, xyz, loop_offsets, nloops, pairs, npairs, h_off, h_all, &d_xyz, &d_off);
+    // Seeded sample of the pairs.
+    const int64_t want = sample_pairs > 0 ? sample_pairs : 2048;
+    std::vector<int64_t> idx(npairs);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::mt19937_64 rng(12345);
+    std::shuffle(idx.begin(), idx.end(), rng);
+    idx.resize(std::min(want, npairs));
+    std::sort(idx.begin(), idx.end());
+    std::vector<int32_t> h_pairs(2 * idx.size());
+    for (size_t k = 0; k < idx.size(); ++k) {
+      h_pairs[2 * k] = h_all[2 * idx[k]];
+      h_pairs[2 * k + 1] = h_all[2 * idx[k] + 1];
+    }
+    const int64_t np = (int64_t)idx.size();
+    double *d_lk = c.d_lk.as<double>(np), *d_err = c.d_err.as<double>(np);
+    int32_t *d_fl = c.d_flags.as<int32_t>(np);
+    auto time_of = [&](const fln_params &p) {
+      double best = 1e300;
+      for (int rep = 0; rep < 2; ++rep) {
+        FLN_CUDA(cudaEventRecord(c.ev0, c.stream));
+        run_pairs(c, d_xyz, d_off, h_off, h_pairs, FLN_METHOD_BARNESHUT, p, d_lk, d_err, d_fl);
+        FLN_CUDA(cudaEventRecord(c.ev1, c.stream));
+        best = std::min(best, (double)c.elapsed(c.ev0, c.ev1));
+      }
+      return best;
+    };
+    time_of(base);  // warm-up: trees, buffers, kernel loading
+    fln_tune_result r{};
+    r.sample_pairs = (int32_t)np;
+    r.default_ms = time_of(base);
+    fln_params best = base;
+    r.best_ms = r.default_ms;
+    r.trials = 1;
+    const double betas[] = {1.5, 2.0, 2.5, 3.0};
+    const int budgets[] = {128, 256, 512};
+    for (double b : betas) {
+      if (!tune_beta && b != base.barnes_hut_init_beta) continue;
+      for (int bud : budgets) {
+        fln_params p = base;
+        if (tune_beta) p.barnes_hut_init_beta = b;
+        p.bh_budget = bud;
+        const double ms = time_of(p);
+        ++r.trials;
+        if (ms < r.best_ms) {
+          r.best_ms = ms;
+          best = p;
+        }
+      }
+    }
+    if (!tune_beta && base.barnes_hut_init_beta != 1.5 && base.barnes_hut_init_beta != 2.0 &&
+        base.barnes_hut_init_beta != 2.5 && base.barnes_hut_init_beta != 3.0)
+      for (int bud : budgets) {  // the caller's own beta
+        fln_params p = base;
+        p.bh_budget = bud;
+        const double ms = time_of(p);
+        ++r.trials;
+        if (ms < r.best_ms) {
+          r.best_ms = ms;
+          best = p;
+        }
+      }
+    r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
+    r.best_beta = best.barnes_hut_init_beta;
+    *out = best;
+    if (result) *result = r;
   });
 }
 

@@ -88,7 +88,10 @@ typedef struct fln_params {
                                    2 = budgeted rounds, evaluation in separate streaming kernels */
   int32_t host_prepare;         /* fln_certificate_compute: 0 = Discretize and the potential-link searches
                                    on the context's GPU (default), 1 = on the host; same output bit for bit */
-  int32_t reserved[2];
+  int32_t bh_budget;            /* traversal steps a warp spends on a batch per launch before handing the
+                                   rest on; 0 = 256. The node pairs stay the same; only the grouping of
+                                   the FP64 partial sums changes (last-bit differences). */
+  int32_t reserved[1];
 } fln_params;
 
 /* Statistics of the last computation on a context. */
@@ -262,6 +265,29 @@ fln_status fln_learned_predict(fln_ctx *ctx, const float *params, const float *f
 fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float *features,
                                  const float *targets, int64_t n, double quantile, float *grad_out,
                                  double *loss_out);
+
+/* ---- Autotuner of the Barnes–Hut stage. No counterpart in the reference.
+ * Times the stage (tree build, traversal, retry, escalation, margin check)
+ * on a seeded sample of the given pairs, `sample_pairs` of them (0 = 2048;
+ * all pairs when there are fewer), for each traversal round budget
+ * {128, 256, 512} and, when tune_beta != 0, each initial beta
+ * {1.5, 2, 2.5, 3} (beta changes the real sums within the Barnes-Hut error,
+ * never the certificate). *out gets *params with the fastest setting;
+ * *result the sample times (device time, best of two runs each). */
+typedef struct fln_tune_result {
+  double best_ms;     /* sample time of the chosen setting */
+  double default_ms;  /* sample time of *params as given */
+  int32_t trials;     /* settings timed */
+  int32_t sample_pairs;
+  int32_t best_budget;
+  int32_t reserved0;
+  double best_beta;
+  double reserved[3];
+} fln_tune_result;
+
+fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                        const int32_t *pairs, int64_t npairs, const fln_params *params, int32_t tune_beta,
+                        int64_t sample_pairs, fln_params *out, fln_tune_result *result);
 
 /* One pair, host arrays (compute_link.h:62-64 and :86-87). */
 fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const double *xyz2,

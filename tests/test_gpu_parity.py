@@ -225,3 +225,23 @@ def test_traversal_schedules_agree(engine, name, golden_dir):
         assert np.array_equal(np.rint(lk), np.rint(lk0))
         np.testing.assert_allclose(lk, lk0, rtol=0, atol=0.05)
         assert s["bh_wait_timeouts"] == 0
+
+
+def test_autotune_budget_keeps_results(engine):
+    # The round budget changes only how work is handed between launches: the
+    # same node pairs, grouped differently into FP64 partial sums (1e-9).
+    off, xyz = workloads.polymer(seed=61, n_loops=30, n_steps=20_000, cube=250.0)
+    m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
+    poff, pxyz, pairs, _ = m.Prepare(True, engine=engine)
+    tuned, res = engine.autotune(pxyz, poff, pairs, sample_pairs=64)
+    assert res["trials"] == 4 and res["sample_pairs"] == min(64, len(pairs))
+    assert tuned.bh_budget in (128, 256, 512) and tuned.barnes_hut_init_beta == 2.0
+    assert res["best_ms"] <= res["default_ms"]
+    lk0, err0, fl0 = engine.linking_numbers(pxyz, poff, pairs, "barneshut")
+    lk1, err1, fl1 = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tuned)
+    np.testing.assert_allclose(lk1, lk0, rtol=0, atol=1e-9)
+    np.testing.assert_array_equal(fl1, fl0)
+    tb, rb = engine.autotune(pxyz, poff, pairs, tune_beta=True, sample_pairs=64)
+    assert rb["trials"] == 13 and tb.barnes_hut_init_beta in (1.5, 2.0, 2.5, 3.0)
+    lk2, _, _ = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tb)
+    assert np.array_equal(np.rint(lk2), np.rint(lk0))
