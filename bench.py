@@ -81,6 +81,7 @@ def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000, en
     t0 = time.perf_counter()
     poff, pxyz, pairs, rounds = m.Prepare(True, engine=engine)
     cfg["prepare_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+    cfg["_raw"] = (off, xyz)  # the curves before Discretize (popped before printing)
     cfg["prepare_on"] = "host" if engine is None else "gpu"
     cfg["discretize_rounds"] = int(rounds)
     cfg["segments_after_discretize"] = int(poff[-1])
@@ -159,6 +160,7 @@ def run_reference(args, rank):
     if rank != 0:
         return
     poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed, args.loops, args.loop_steps)
+    cfg.pop("_raw", None)
     from oracle import pyoracle
     threads = pyoracle.max_threads()
     vals = []
@@ -196,6 +198,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     eng = Engine(local_rank, stream.cuda_stream)
     poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank, args.loops, args.loop_steps, engine=eng)
+    raw_curves = cfg.pop("_raw")
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
                            bh_tree=args.bh_tree, bh_schedule=args.bh_schedule)
     tune = None
@@ -366,6 +369,25 @@ def run_ours(args, rank, world, local_rank):
             "same_integers_as_plain": bool(np.array_equal(np.round(llk), np.round(lk))),
             "max_abs_diff_vs_plain": float(np.abs(llk - lk).max()),
         }
+    if rank == 0 and world == 1 and args.cli_leg:
+        # End to end through the flag-compatible CLI: a fresh process loads
+        # the BCC, prepares on the GPU, runs Barnes-Hut and writes the
+        # certificate (wall clock, so it includes CUDA start-up).
+        from fastlinkingnumbers_b200 import workloads as W
+        from fastlinkingnumbers_b200._native import LIB_DIR
+        with tempfile.TemporaryDirectory() as td:
+            path, cert = os.path.join(td, "w.bcc"), os.path.join(td, "cert.txt")
+            W.write_bcc(path, raw_curves)
+            walls = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                subprocess.run([os.path.join(LIB_DIR, "verifycurves"), "--input", path, "--output", cert],
+                               check=True, capture_output=True)
+                walls.append(round(time.perf_counter() - t0, 3))
+            entries = len(open(cert).read().strip().splitlines()) - 1
+        result["cli_e2e"] = {"command": "verifycurves --input <workload>.bcc --output cert.txt",
+                             "wall_s": walls, "certificate_entries": entries,
+                             "same_entry_count_as_bench": entries == int(np.sum(np.round(lk) != 0))}
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         from oracle import pyoracle
         thr = pyoracle.max_threads()
@@ -399,6 +421,8 @@ def main():
     ap.add_argument("--direct-sample", type=int, default=64)
     ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=67.0,
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
+    ap.add_argument("--cli-leg", type=int, default=1,
+                    help="also time the verifycurves CLI end to end on the workload written as BCC")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune the Barnes-Hut round budget on a sample of the pairs before timing")
     ap.add_argument("--learned-leg", type=int, default=1,
