@@ -202,7 +202,9 @@ def run_ours(args, rank, world, local_rank):
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
                            bh_tree=args.bh_tree, bh_schedule=args.bh_schedule)
     tune = None
-    if args.autotune and args.method == "barneshut":
+    if args.bh_budget:
+        prm.bh_budget = args.bh_budget
+    elif args.autotune and args.method == "barneshut":
         # Round budget only: the same node pairs, so results change only in the
         # rounding of partial sums (beta stays the reference's 2). Tuned on a
         # seeded sample of the pairs, untimed.
@@ -419,10 +421,12 @@ def main():
     ap.add_argument("--loop-steps", type=int, default=50000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
-    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=67.0,
+    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=59.6,
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
     ap.add_argument("--cli-leg", type=int, default=1,
                     help="also time the verifycurves CLI end to end on the workload written as BCC")
+    ap.add_argument("--bh-budget", type=int, default=0,
+                    help="fixed Barnes-Hut round budget (skips the autotuner); 0 = tuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune the Barnes-Hut round budget on a sample of the pairs before timing")
     ap.add_argument("--learned-leg", type=int, default=1,

@@ -82,6 +82,15 @@ __device__ __forceinline__ int find_curve(const int64_t *start, int n, int64_t x
 // Order-preserving key of a non-negative double (NaN above +inf).
 __device__ __forceinline__ unsigned long long dkey(double v) { return (unsigned long long)__double_as_longlong(v); }
 
+// count[key] += 1 for the calling lane, one atomic per distinct key of the
+// warp (neighbouring pieces mostly belong to the same curve).
+__device__ __forceinline__ void add_one(int32_t *count, int32_t key, bool active) {
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  const unsigned peers = __match_any_sync(act, key);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&count[key], __popc(peers));
+}
+
 __global__ void init_pieces(const int64_t *seg_off, int nc, int64_t total, Pieces P) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
@@ -101,9 +110,9 @@ __global__ void flag_live(const uint8_t *live, int64_t n, int32_t *flag) {
 __global__ void compact_live(const uint8_t *live, const int32_t *pos, const int32_t *curve, int64_t n, int32_t *lidx,
                              int32_t *count_per_curve) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n || !live[k]) return;
-  lidx[pos[k]] = (int32_t)k;
-  atomicAdd(&count_per_curve[curve[k]], 1);
+  const bool on = k < n && live[k];
+  if (on) lidx[pos[k]] = (int32_t)k;
+  add_one(count_per_curve, on ? curve[k] : 0, on);
 }
 
 // Leaf records of the live pieces: the piece box and its range; the minimum
@@ -382,7 +391,7 @@ __global__ void refine(Pieces S, const uint8_t *hit, const int32_t *pos, int64_t
 
 __global__ void count_per_curve(const int32_t *pc, int64_t n, int32_t *cnt) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) atomicAdd(&cnt[pc[k]], 1);
+  add_one(cnt, k < n ? pc[k] : 0, k < n);
 }
 
 // Output vertex of every piece (its start point).
