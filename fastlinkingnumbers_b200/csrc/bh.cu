@@ -71,13 +71,33 @@ constexpr int kSpill = 8192;       // global spill entries per warp
 #endif
 
 // FP64 build record.
-struct BuildNode {
+struct __align__(16) BuildNode {
   double lo[3], hi[3];
   double mid[3];
   double t[3];
   double D[9];   // row-major
   double Q[18];  // Q_k symmetric: (xx, yy, zz, xy, xz, yz) for k = 0, 1, 2
+  double pad;    // 320 B: whole 16-byte vectors
 };
+static_assert(sizeof(BuildNode) == 320, "BuildNode layout");
+
+// Record copies as 16-byte vectors (a thread's record is contiguous; with
+// field-by-field stores every warp instruction would touch 32 lines).
+template <class T>
+__device__ __forceinline__ void put16(T *dst, const T &src) {
+  static_assert(sizeof(T) % 16 == 0 && alignof(T) >= 16, "16-byte record");
+  const int4 *s = reinterpret_cast<const int4 *>(&src);
+  int4 *d = reinterpret_cast<int4 *>(dst);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 16); ++i) d[i] = s[i];
+}
+template <class T>
+__device__ __forceinline__ void get16(const T *src, T &dst) {
+  const int4 *s = reinterpret_cast<const int4 *>(src);
+  int4 *d = reinterpret_cast<int4 *>(&dst);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 16); ++i) d[i] = s[i];
+}
 
 // Traversal records.
 struct __align__(16) NodeHdr {
@@ -122,10 +142,46 @@ __device__ __forceinline__ int find_loop_of(const int64_t *start, int n, int64_t
   return lo;
 }
 
+// count[key] += 1 for the calling lane, one atomic per distinct key of the
+// warp; returns the count before the warp's run plus the lane's rank among
+// the lanes of the warp with its key.
+__device__ __forceinline__ int32_t add_one_rank(int32_t *count, int32_t key, bool active) {
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!active) return 0;
+  const unsigned peers = __match_any_sync(act, key);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  int32_t base = 0;
+  if (lane == leader) base = atomicAdd(&count[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1));
+}
+
 // Curve-order topology: thread per internal node (local id s - 1 splits at s).
-// seg_start[k] = sum of (n - 1) over the first k listed loops.
-__global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t total_internal) {
+// seg_start[k] = sum of (n - 1) over the first k listed loops. With height
+// != nullptr it also records the node's height ceil(log2(range size)) (the
+// children of a node are always lower) and counts the nodes per height.
+__global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t total_internal, uint8_t *height,
+                                    int32_t *height_count) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (height) {  // every lane of the warp takes part in the counting
+    int32_t h = 0;
+    if (g < total_internal) {
+      const int k = find_loop_of(seg_start, A.nloops, g);
+      const int l = A.loops[k];
+      const int64_t n = A.off[l + 1] - A.off[l];
+      const int64_t s = g - seg_start[k] + 1;
+      int64_t lo = 0, hi = n;
+      for (int depth = 0; depth < 64; ++depth) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (mid == s) break;
+        if (s < mid) hi = mid;
+        else lo = mid;
+      }
+      h = 64 - __clzll((unsigned long long)(hi - lo - 1));
+      height[g] = (uint8_t)h;
+    }
+    add_one_rank(height_count, h, g < total_internal);
+  }
   if (g >= total_internal) return;
   const int k = find_loop_of(seg_start, A.nloops, g);
   const int l = A.loops[k];
@@ -189,8 +245,8 @@ __device__ void accumulate_child(BuildNode &P, const BuildNode &C) {
     }
 }
 
-__device__ void finish_record(const BuildNode &B, NodeHdr &H, NodeMom &M, bool leaf, int32_t seg, int32_t l,
-                              int32_t r) {
+__device__ void finish_record_regs(const BuildNode &B, NodeHdr &H, NodeMom &M, bool leaf, int32_t seg, int32_t l,
+                                   int32_t r) {
   const double dx = B.hi[0] - B.lo[0], dy = B.hi[1] - B.lo[1], dz = B.hi[2] - B.lo[2];
   H.m[0] = B.mid[0];
   H.m[1] = B.mid[1];
@@ -212,6 +268,16 @@ __device__ void finish_record(const BuildNode &B, NodeHdr &H, NodeMom &M, bool l
   // Leaf: |c|^3 / 36, which is also (1/3) ||C_Q||_F for c c c^T / 12.
   M.qn = (float)(leaf ? tn * tn * tn / 36.0 : sqrt(qq) / 3.0);
   M.pad[0] = M.pad[1] = M.pad[2] = 0.f;
+}
+
+// Traversal records of a node, formed in registers and stored as vectors.
+__device__ __forceinline__ void finish_record(const BuildNode &B, NodeHdr &H, NodeMom &M, bool leaf, int32_t seg,
+                                              int32_t l, int32_t r) {
+  NodeHdr h;
+  NodeMom m;
+  finish_record_regs(B, h, m, leaf, seg, l, r);
+  put16(&H, h);
+  put16(&M, m);
 }
 
 // Leaf record of segment `seg` of a loop at vertex offset o with n segments
@@ -237,10 +303,10 @@ __device__ void leaf_build(const double *xyz, int64_t o, int64_t n, int32_t seg,
 // Thread per leaf: write the leaf's traversal record and walk up; the second
 // child to arrive at a parent builds it. Leaf build records are never
 // stored: a parent rebuilds a leaf child from its two vertices (48 B read
-// instead of a 312 B record written and read back). The arrival counter is
+// instead of a 320 B record written and read back). The arrival counter is
 // an acquire-release atomic, which orders the first child's record before
 // the second child's reads.
-__global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t total) {
+__global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t total, bool walk_up) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
   const int k = find_loop_of(seg_start2, A.nloops, g);
@@ -255,6 +321,7 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
     finish_record(B, A.hdr[base + node], A.mom[base + node], true, seg, 0, 0);
   }
   const int32_t first_leaf = (int32_t)(n - 1);
+  if (!walk_up) return;
   for (int guard = 0; guard < 128; ++guard) {
     const int32_t par = A.parent[base + node];
     if (par < 0) break;
@@ -281,6 +348,50 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
     finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
     node = par;
   }
+}
+
+// Level-synchronous build of curve-order trees: the internal nodes of one
+// height, listed in bucket[0, count), each from its two children, which
+// earlier launches finished (leaves: rebuilt from their vertices). Same
+// arithmetic as the walk-up of build_moments, so the same records.
+__global__ void bucket_heights(const uint8_t *height, int64_t total_internal, const int32_t *height_off,
+                               int32_t *cursor, int32_t *bucket) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t h = g < total_internal ? height[g] : 0;
+  const int32_t r = add_one_rank(cursor, h, g < total_internal);
+  if (g < total_internal) bucket[height_off[h] + r] = (int32_t)g;
+}
+
+__global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const int64_t g = bucket[e];
+  const int k = find_loop_of(seg_start, A.nloops, g);
+  const int l = A.loops[k];
+  const int64_t o = A.off[l], n = A.off[l + 1] - o;
+  const int64_t base = A.node_base[l];
+  const int32_t par = (int32_t)(g - seg_start[k]);
+  const int32_t first_leaf = (int32_t)(n - 1);
+  const int32_t cl = A.children[2 * (base + par)], cr = A.children[2 * (base + par) + 1];
+  BuildNode L, R;
+  if (cl >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cl], L);
+  else get16(A.bn + base + cl, L);
+  if (cr >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cr], R);
+  else get16(A.bn + base + cr, R);
+  BuildNode P;
+  for (int a = 0; a < 3; ++a) {
+    P.lo[a] = fmin(L.lo[a], R.lo[a]);
+    P.hi[a] = fmax(L.hi[a], R.hi[a]);
+    P.mid[a] = 0.5 * (P.hi[a] + P.lo[a]);
+    P.t[a] = 0.0;
+  }
+  for (int a = 0; a < 9; ++a) P.D[a] = 0.0;
+  for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
+  accumulate_child(P, L);
+  accumulate_child(P, R);
+  P.pad = 0.0;
+  put16(A.bn + base + par, P);
+  finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
 }
 
 // ------------------------------------------------------------------ traversal
@@ -1665,16 +1776,45 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
                                                                         d_segint, tot_int, d_parent, d_arrive);
     FLN_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
     ++launches;
+    build_moments<<<(int)((tot_leaf + 127) / 128), 128, 0, st>>>(T, d_segall, tot_leaf, true);
+    FLN_CUDA(cudaGetLastError());
+    ++launches;
   } else {
-    curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int);
+    // Curve-order trees: topology with node heights, leaf records, then one
+    // launch per height (no arrival counters, no serial walk-up chains).
+    uint8_t *d_height = ctx.d_bh[20].as<uint8_t>(std::max<int64_t>(tot_int, 1));
+    int32_t *d_hcnt = ctx.d_bh[18].as<int32_t>(3 * 64);
+    int32_t *d_hoff = d_hcnt + 64, *d_hcur = d_hcnt + 128;
+    int32_t *d_bucket = ctx.d_bh[19].as<int32_t>(std::max<int64_t>(tot_int, 1));
+    FLN_CUDA(cudaMemsetAsync(d_hcnt, 0, 3 * 64 * sizeof(int32_t), st));
+    if (tot_int > 0)
+      curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int, d_height, d_hcnt);
     identity_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
-    launches += 2;
+    build_moments<<<(int)((tot_leaf + 127) / 128), 128, 0, st>>>(T, d_segall, tot_leaf, false);
+    FLN_CUDA(cudaGetLastError());
+    launches += 3;
+    int32_t hcnt[64];
+    FLN_CUDA(cudaMemcpyAsync(hcnt, d_hcnt, sizeof hcnt, cudaMemcpyDeviceToHost, st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+    int32_t hoff[64];
+    int32_t acc = 0;
+    for (int h = 0; h < 64; ++h) {
+      hoff[h] = acc;
+      acc += hcnt[h];
+    }
+    if (tot_int > 0) {
+      FLN_CUDA(cudaMemcpyAsync(d_hoff, hoff, sizeof hoff, cudaMemcpyHostToDevice, st));
+      bucket_heights<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(d_height, tot_int, d_hoff, d_hcur, d_bucket);
+      ++launches;
+      for (int h = 1; h < 64; ++h) {
+        if (!hcnt[h]) continue;
+        build_height<<<(hcnt[h] + 127) / 128, 128, 0, st>>>(T, d_segint, d_bucket + hoff[h], hcnt[h]);
+        ++launches;
+      }
+      FLN_CUDA(cudaGetLastError());
+    }
   }
-  FLN_CUDA(cudaGetLastError());
-  build_moments<<<(int)((tot_leaf + 127) / 128), 128, 0, st>>>(T, d_segall, tot_leaf);
-  FLN_CUDA(cudaGetLastError());
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
-  ++launches;
   ctx.stats.ms_tree_build = ctx.elapsed(ctx.ev2, ctx.ev3);
 
   // Slots: pairs ordered by decreasing estimated work.
