@@ -127,9 +127,10 @@ struct TreeArgs {
   int32_t *parent;           // per global node
   int32_t *leaf_seg;         // per global node: segment of a leaf (kd trees permute)
   int32_t *arrive;           // per global node: arrival counter
-  BuildNode *bn;
+  BuildNode *bn;              // per internal node: bn[int_start[k] + id] for the k-th listed loop
   NodeHdr *hdr;
   NodeMom *mom;
+  const int64_t *int_start;   // listed loop -> first build record (sum of (n - 1) before it)
 };
 
 __device__ __forceinline__ int find_loop_of(const int64_t *start, int n, int64_t x) {
@@ -330,9 +331,9 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
     const int32_t cl = A.children[2 * (base + par)], cr = A.children[2 * (base + par) + 1];
     BuildNode L, R;
     if (cl >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cl], L);
-    else load_cg(A.bn + base + cl, L);
+    else load_cg(A.bn + A.int_start[k] + cl, L);
     if (cr >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cr], R);
-    else load_cg(A.bn + base + cr, R);
+    else load_cg(A.bn + A.int_start[k] + cr, R);
     BuildNode P;
     for (int a = 0; a < 3; ++a) {
       P.lo[a] = fmin(L.lo[a], R.lo[a]);
@@ -344,7 +345,7 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
     for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
     accumulate_child(P, L);
     accumulate_child(P, R);
-    A.bn[base + par] = P;
+    A.bn[A.int_start[k] + par] = P;
     finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
     node = par;
   }
@@ -375,9 +376,9 @@ __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t
   const int32_t cl = A.children[2 * (base + par)], cr = A.children[2 * (base + par) + 1];
   BuildNode L, R;
   if (cl >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cl], L);
-  else get16(A.bn + base + cl, L);
+  else get16(A.bn + seg_start[k] + cl, L);
   if (cr >= first_leaf) leaf_build(A.xyz, o, n, A.leaf_seg[base + cr], R);
-  else get16(A.bn + base + cr, R);
+  else get16(A.bn + seg_start[k] + cr, R);
   BuildNode P;
   for (int a = 0; a < 3; ++a) {
     P.lo[a] = fmin(L.lo[a], R.lo[a]);
@@ -390,7 +391,7 @@ __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t
   accumulate_child(P, L);
   accumulate_child(P, R);
   P.pad = 0.0;
-  put16(A.bn + base + par, P);
+  put16(A.bn + g, P);
   finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
 }
 
@@ -1744,7 +1745,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   int32_t *d_parent = ctx.d_bh[5].as<int32_t>(nodes);
   int32_t *d_leafseg = ctx.d_bh[6].as<int32_t>(nodes);
   int32_t *d_arrive = ctx.d_bh[7].as<int32_t>(nodes);
-  BuildNode *d_bn = ctx.d_bh[8].as<BuildNode>(nodes);
+  BuildNode *d_bn = ctx.d_bh[8].as<BuildNode>(std::max<int64_t>(tot_int, 1));  // internal nodes only
   NodeHdr *d_hdr = ctx.d_bh[9].as<NodeHdr>(nodes);
   NodeMom *d_mom = ctx.d_bh[10].as<NodeMom>(nodes);
   cudaStream_t st = ctx.stream;
@@ -1752,7 +1753,8 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_base, node_base.data(), nl_all * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_segint, seg_int.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_segall, seg_all.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-  TreeArgs T{d_xyz, d_off, d_base, d_loops, nloops, d_children, d_parent, d_leafseg, d_arrive, d_bn, d_hdr, d_mom};
+  TreeArgs T{d_xyz, d_off, d_base, d_loops, nloops, d_children, d_parent, d_leafseg, d_arrive, d_bn, d_hdr, d_mom,
+             d_segint};
   int launches = 0;
   FLN_CUDA(cudaEventRecord(ctx.ev2, st));
   if (prm.bh_tree == 1) {

@@ -779,6 +779,10 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
     pairs_out[2 * k] = pl[k].first;
     pairs_out[2 * k + 1] = pl[k].second;
   }
+  // The working buffers (tens of GB for 10^8 segments) are not kept for the
+  // linking-number stage that follows.
+  FLN_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < 34; ++k) B[k].release();
 }
 
 }  // namespace fln
