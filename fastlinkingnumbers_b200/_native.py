@@ -66,7 +66,7 @@ class Params(C.Structure):
         ("precision", C.c_int32), ("fp64_margin", C.c_double), ("near_factor", C.c_double),
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
         ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("bh_budget", C.c_int32),
-        ("reserved", C.c_int32 * 1),
+        ("bh_bucket", C.c_int32),
     ]
 
 

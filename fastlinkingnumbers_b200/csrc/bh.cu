@@ -66,6 +66,9 @@ constexpr int kWarps = 4;          // warps per traversal CTA
 #endif
 constexpr int kStack = FLN_BH_STACK;
 constexpr int kSpill = 8192;       // global spill entries per warp
+#ifndef FLN_BUCKET_SOFT_LOG2
+#define FLN_BUCKET_SOFT_LOG2 19  // exact-list chunks per round before it stops taking batches
+#endif
 #ifndef FLN_CHUNK_SOFT_LOG2
 #define FLN_CHUNK_SOFT_LOG2 20  // chunks per list before a round stops taking batches
 #endif
@@ -77,7 +80,7 @@ struct __align__(16) BuildNode {
   double t[3];
   double D[9];   // row-major
   double Q[18];  // Q_k symmetric: (xx, yy, zz, xy, xz, yz) for k = 0, 1, 2
-  double pad;    // 320 B: whole 16-byte vectors
+  int32_t seg_lo, seg_cnt;  // leaves below: a curve-order node covers segments [seg_lo, seg_lo + seg_cnt)
 };
 static_assert(sizeof(BuildNode) == 320, "BuildNode layout");
 
@@ -106,8 +109,11 @@ struct __align__(16) NodeHdr {
   double rsq;       // its square, 0.25 |diag|^2, for the reference's split rule
   int32_t left;     // internal: local child ids; leaf: left = -1 - segment
   int32_t right;
+  int32_t lo;       // leaf: its segment; curve-order node: first segment of its range
+  int32_t cnt;      // leaves below (curve-order: the range is [lo, lo + cnt))
+  int32_t pad[2];   // 64 B: a record never straddles a 128 B line
 };
-static_assert(sizeof(NodeHdr) == 48, "NodeHdr layout");
+static_assert(sizeof(NodeHdr) == 64, "NodeHdr layout");
 struct __align__(16) NodeMom {
   float t[3];
   float D[9];
@@ -256,6 +262,9 @@ __device__ void finish_record_regs(const BuildNode &B, NodeHdr &H, NodeMom &M, b
   H.r = sqrt(H.rsq);
   H.left = leaf ? -1 - seg : l;
   H.right = leaf ? -1 : r;
+  H.lo = B.seg_lo;
+  H.cnt = B.seg_cnt;
+  H.pad[0] = H.pad[1] = 0;
   const double tn = sqrt(B.t[0] * B.t[0] + B.t[1] * B.t[1] + B.t[2] * B.t[2]);
   double dd = 0, qq = 0;
   for (int a = 0; a < 9; ++a) dd += B.D[a] * B.D[a];
@@ -295,6 +304,8 @@ __device__ void leaf_build(const double *xyz, int64_t o, int64_t n, int32_t seg,
     B.mid[a] = 0.5 * p0[a] + 0.5 * p1[a];
     B.t[a] = p1[a] - p0[a];
   }
+  B.seg_lo = seg;
+  B.seg_cnt = 1;
   for (int a = 0; a < 9; ++a) B.D[a] = 0.0;
   const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
   for (int kk = 0; kk < 3; ++kk)
@@ -345,6 +356,8 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
     for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
     accumulate_child(P, L);
     accumulate_child(P, R);
+    P.seg_lo = L.seg_lo;
+    P.seg_cnt = L.seg_cnt + R.seg_cnt;
     A.bn[A.int_start[k] + par] = P;
     finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
     node = par;
@@ -390,12 +403,25 @@ __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t
   for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
   accumulate_child(P, L);
   accumulate_child(P, R);
-  P.pad = 0.0;
+  P.seg_lo = L.seg_lo;
+  P.seg_cnt = L.seg_cnt + R.seg_cnt;
   put16(A.bn + g, P);
   finish_record(P, A.hdr[base + par], A.mom[base + par], false, 0, cl, cr);
 }
 
 // ------------------------------------------------------------------ traversal
+// Node pairs summed exactly, segment pair by segment pair: leaf pairs, and
+// pairs that are neither far nor larger than `bucket` segments a side.
+// Entry: first segment and segment count of each node (curve-order ranges;
+// a leaf is its own segment, count 1). All entries of a chunk belong to one
+// loop pair (slot).
+struct BucketChunk {
+  int32_t slot;
+  int32_t count;
+  int32_t pad[2];
+  int4 e[32];  // lo1, lo2, cnt1, cnt2
+};
+
 // A unit of traversal work: up to 32 node pairs of one loop pair (slot).
 struct Batch {
   int32_t slot;
@@ -418,6 +444,10 @@ struct TravArgs {
   int64_t out_cap;
   unsigned long long *out_count;
   int32_t budget;              // iterations per batch before its stack is handed on
+  int32_t bucket;              // node pairs of at most this many segments a side are summed exactly
+  BucketChunk *bkt;            // exact node pairs, handed to bh_buckets
+  unsigned long long *bkt_count;
+  int64_t bkt_soft, bkt_cap;   // no new batch past soft; hard capacity
   unsigned long long *acc_lk;  // per slot, fixed point (2^-40 turns)
   unsigned long long *acc_err; // per slot, fixed point (2^-40)
   double *counts;              // [0] far evals, [1] leaf evals
@@ -584,25 +614,19 @@ __device__ __noinline__ double seg_term_fp64(const double *xyz, int64_t p0i, int
   return kInvTwoPi * atan2(y, x) + (((s < 0) || ((s == 0) && (det < 0))) ? sg : 0.0);
 }
 
-// Exact leaf-leaf term in FP32 from the separation and the two tangents
-// (compute_link.cpp:576-606); FP64 from the vertices when the segments are
-// closer than their length.
-__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &m1,
-                          const NodeMom &m2, int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
-  const float rx = (float)(h2.m[0] - h1.m[0]), ry = (float)(h2.m[1] - h1.m[1]), rz = (float)(h2.m[2] - h1.m[2]);
-  const float t1x = m1.t[0], t1y = m1.t[1], t1z = m1.t[2];
-  const float t2x = m2.t[0], t2y = m2.t[1], t2z = m2.t[2];
+// Exact segment-pair term in FP32 (compute_link.cpp:576-606) from the
+// midpoint separation r and the two segment vectors; false (nothing added)
+// when the segments are closer than the longer one's length, where the
+// caller evaluates the pair in FP64 from its vertices.
+__device__ __forceinline__ bool seg_term_fp32(float rx, float ry, float rz, float t1x, float t1y, float t1z,
+                                              float t2x, float t2y, float t2z, float tnmax, double &sum) {
   const float alx = rx + 0.5f * (t1x - t2x), aly = ry + 0.5f * (t1y - t2y), alz = rz + 0.5f * (t1z - t2z);
   const float bex = rx - 0.5f * (t2x + t1x), bey = ry - 0.5f * (t2y + t1y), bez = rz - 0.5f * (t2z + t1z);
   const float gax = rx + 0.5f * (t2x - t1x), gay = ry + 0.5f * (t2y - t1y), gaz = rz + 0.5f * (t2z - t1z);
   const float dex = rx + 0.5f * (t2x + t1x), dey = ry + 0.5f * (t2y + t1y), dez = rz + 0.5f * (t2z + t1z);
   const float la = sqrtf(dot3(alx, aly, alz, alx, aly, alz)), lb = sqrtf(dot3(bex, bey, bez, bex, bey, bez));
   const float lc = sqrtf(dot3(gax, gay, gaz, gax, gay, gaz)), ld = sqrtf(dot3(dex, dey, dez, dex, dey, dez));
-  if (fminf(fminf(la, lb), fminf(lc, ld)) < fmaxf(m1.tn, m2.tn)) {
-    const int64_t s1 = -1 - h1.left, s2 = -1 - h2.left;
-    sum += seg_term_fp64(xyz, o1 + s1, o1 + (s1 + 1 == n1 ? 0 : s1 + 1), o2 + s2, o2 + (s2 + 1 == n2 ? 0 : s2 + 1));
-    return;
-  }
+  if (fminf(fminf(la, lb), fminf(lc, ld)) < tnmax) return false;
   const float det = rx * (t2y * t1z - t2z * t1y) + ry * (t2z * t1x - t2x * t1z) + rz * (t2x * t1y - t2y * t1x);
   const float ac = dot3(alx, aly, alz, gax, gay, gaz);
   const float div1 = la * lb * lc + dot3(alx, aly, alz, bex, bey, bez) * lc + ac * lb + dot3(bex, bey, bez, gax, gay, gaz) * la;
@@ -612,6 +636,41 @@ __device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h
   const float y = det * s;
   const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
   sum += kInvTwoPi * (double)atan2f(y, x) + (((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? (double)sg : 0.0);
+  return true;
+}
+
+// Exact leaf-leaf term from the two leaf records (midpoints, tangents); the
+// same value as seg_pair_eval of the two segments.
+__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &m1,
+                          const NodeMom &m2, int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
+  const float rx = (float)(h2.m[0] - h1.m[0]), ry = (float)(h2.m[1] - h1.m[1]), rz = (float)(h2.m[2] - h1.m[2]);
+  // The near test of seg_pair_eval, from the same FP32 segment vectors.
+  const float tn = sqrtf(fmaxf(dot3(m1.t[0], m1.t[1], m1.t[2], m1.t[0], m1.t[1], m1.t[2]),
+                               dot3(m2.t[0], m2.t[1], m2.t[2], m2.t[0], m2.t[1], m2.t[2])));
+  if (seg_term_fp32(rx, ry, rz, m1.t[0], m1.t[1], m1.t[2], m2.t[0], m2.t[1], m2.t[2], tn, sum)) return;
+  const int64_t s1 = -1 - h1.left, s2 = -1 - h2.left;
+  sum += seg_term_fp64(xyz, o1 + s1, o1 + (s1 + 1 == n1 ? 0 : s1 + 1), o2 + s2, o2 + (s2 + 1 == n2 ? 0 : s2 + 1));
+}
+
+// Exact term of segment s1 of loop 1 and segment s2 of loop 2 from their
+// vertices: midpoints and segment vectors in FP64 as the leaf records form
+// them (halving is exact, so the midpoint rounds once either way), the term
+// in FP32 (FP64 for close segments).
+__device__ __forceinline__ void seg_pair_eval(const double *xyz, int64_t o1, int64_t n1, int32_t s1, int64_t o2,
+                                              int64_t n2, int32_t s2, double &sum) {
+  const int64_t a0 = o1 + s1, a1 = o1 + (s1 + 1 == n1 ? 0 : s1 + 1);
+  const int64_t b0 = o2 + s2, b1 = o2 + (s2 + 1 == n2 ? 0 : s2 + 1);
+  float r[3], t1[3], t2[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double p0 = xyz[3 * a0 + a], p1 = xyz[3 * a1 + a], q0 = xyz[3 * b0 + a], q1 = xyz[3 * b1 + a];
+    r[a] = (float)((0.5 * q0 + 0.5 * q1) - (0.5 * p0 + 0.5 * p1));
+    t1[a] = (float)(p1 - p0);
+    t2[a] = (float)(q1 - q0);
+  }
+  const float tn = sqrtf(fmaxf(dot3(t1[0], t1[1], t1[2], t1[0], t1[1], t1[2]), dot3(t2[0], t2[1], t2[2], t2[0], t2[1], t2[2])));
+  if (seg_term_fp32(r[0], r[1], r[2], t1[0], t1[1], t1[2], t2[0], t2[1], t2[2], tn, sum)) return;
+  sum += seg_term_fp64(xyz, a0, a1, b0, b1);
 }
 
 // Traversal steps a warp takes on one batch per round before it hands the
@@ -625,6 +684,11 @@ __device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h
 // valid device memory). Bit 0: the next step's headers into L1; bit 1: the
 // moment records of queued far-field and leaf pairs into L1. Same step:
 // none 207.4 ms, bit 1 206.5 ms, bit 0 211.7 ms, both 212.2 ms.
+// Node pairs (neither far nor split further) of at most this many segments
+// a side are summed exactly, segment pair by segment pair.
+#ifndef FLN_BH_BUCKET
+#define FLN_BH_BUCKET 8
+#endif
 #ifndef FLN_BH_PREFETCH
 #define FLN_BH_PREFETCH 2
 #endif
@@ -661,13 +725,11 @@ template <bool kLearn, bool kRecord>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
-  __shared__ int2 s_leaf[kWarps][64];
   __shared__ std::conditional_t<kLearn, MlpFrag, int> s_mlp;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + w;
   int2 *stack = s_stack[w];
   int2 *farq = s_far[w];
-  int2 *leafq = s_leaf[w];
   if constexpr (kLearn) {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(A.learned.frag);
     uint32_t *dst = reinterpret_cast<uint32_t *>(&s_mlp);
@@ -675,10 +737,15 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     __syncthreads();
   }
   int2 *spill = A.spill + (size_t)gw * kSpill;
-  double nfar = 0, nleaf = 0;
+  double nfar = 0;
   for (;;) {
     long long b = 0;
-    if (lane == 0) b = (long long)atomicAdd(A.queue, 1ULL);
+    if (lane == 0) {
+      // Past the soft limit of the exact list this round takes no new batch
+      // (they carry over).
+      const bool full = (int64_t)*(volatile unsigned long long *)A.bkt_count > A.bkt_soft;
+      b = full ? A.nin : (long long)atomicAdd(A.queue, 1ULL);
+    }
     b = __shfl_sync(0xffffffffu, b, 0);
     if (b >= A.nin) break;
     const int slot = A.in[b].slot;
@@ -691,7 +758,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     // Threshold of the learned criterion: tau x (beta0 / beta)^4 in later passes.
     const float log10_tau = A.learned.log10_tau + 2.f * (float)log10(A.beta0 * A.beta0 / itolsq);
     if (lane < cnt0) stack[lane] = A.in[b].pairs[lane];
-    int top = cnt0, nspill = 0, nf = 0, nl = 0, steps = 0;
+    int top = cnt0, nspill = 0, nf = 0, steps = 0;
+    long long bc = -1;  // open chunk of the exact list
+    int bfill = 0;      // entries in it
     bool overflow = false;
     double sum = 0.0, err = 0.0;
     __syncwarp();
@@ -740,7 +809,8 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       if (act) pr = stack[top - cnt + lane];
       __syncwarp();
       top -= cnt;
-      int kind = 0;  // 0 none, 1 leaf, 2 far, 3 split
+      int kind = 0;  // 0 none, 1 exact (leaf pair or bucket), 2 far, 3 split
+      int4 ex = make_int4(0, 0, 1, 1);
       int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
       float sep = 0.f;
       double dsq = 0.0;
@@ -753,8 +823,12 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         sep = (float)(sqrt(dsq) / rs);
         if (leaf1 && leaf2) {
           kind = 1;
+          ex = make_int4(h1.lo, h2.lo, 1, 1);
         } else if (dsq > rs * rs * itolsq + eps) {
           kind = 2;
+        } else if (h1.cnt <= A.bucket && h2.cnt <= A.bucket) {
+          kind = 1;
+          ex = make_int4(h1.lo, h2.lo, h1.cnt, h2.cnt);
         } else {
           kind = 3;
           const bool split2 = (!leaf1 && !leaf2) ? (h2.rsq > h1.rsq) : !leaf2;
@@ -821,15 +895,37 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
       const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
       if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
-      if (kind == 1) leafq[nl + __popc(lm & ((1u << lane) - 1))] = pr;
 #if FLN_BH_PREFETCH & 2
-      if (kind == 1 || kind == 2) {
+      if (kind == 2) {
         prefetch_record(M1 + pr.x);
         prefetch_record(M2 + pr.y);
       }
 #endif
       nf += __popc(fm);
-      nl += __popc(lm);
+      if (lm) {  // append the exact pairs to the list, 32 entries per chunk
+        const int ne = __popc(lm), pos = bfill + __popc(lm & ((1u << lane) - 1));
+        const int need = (bc < 0 ? 1 : 0) + (bfill + ne > 32 ? 1 : 0);
+        long long c = 0;
+        if (lane == 0 && need) c = (long long)atomicAdd(A.bkt_count, (unsigned long long)need);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        const long long cur = bc < 0 ? c : bc, nxt = bc < 0 ? c + 1 : c;
+        const long long dst = pos < 32 ? cur : nxt;
+        if (kind == 1) {
+          if (dst < A.bkt_cap) A.bkt[dst].e[pos & 31] = ex;
+          else atomicOr(A.status, 4);
+        }
+        if (bfill + ne >= 32) {
+          if (lane == 0 && cur < A.bkt_cap) {
+            A.bkt[cur].slot = slot;
+            A.bkt[cur].count = 32;
+          }
+          bc = bfill + ne > 32 ? nxt : -1;
+          bfill = bfill + ne - 32;
+        } else {
+          bc = cur;
+          bfill += ne;
+        }
+      }
       __syncwarp();
 #if FLN_BH_PREFETCH & 1
       {  // the next step's headers, while the queued evaluations run
@@ -851,13 +947,6 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         nf -= 32;
         __syncwarp();
       }
-      while (nl >= 32) {
-        const int2 q = leafq[nl - 32 + lane];
-        leaf_eval(A.xyz, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
-        nleaf += 32;
-        nl -= 32;
-        __syncwarp();
-      }
     }
     // Evaluate what is still queued.
     if (lane < nf) {
@@ -867,12 +956,11 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
                (float)h2.r, sum, err);
     }
-    if (lane < nl) {
-      const int2 q = leafq[lane];
-      leaf_eval(A.xyz, H1[q.x], H2[q.y], M1[q.x], M2[q.y], o1, n1, o2, n2, sum);
+    if (bc >= 0 && lane == 0 && bc < A.bkt_cap) {
+      A.bkt[bc].slot = slot;
+      A.bkt[bc].count = bfill;
     }
     nfar += nf;
-    nleaf += nl;
     __syncwarp();
     if (overflow && lane == 0) atomicExch(A.status, 1);
     for (int o = 16; o; o >>= 1) {
@@ -886,8 +974,67 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
   if (lane == 0) {
     atomicAdd(A.counts, nfar);
-    atomicAdd(A.counts + 1, nleaf);
   }
+}
+
+// Exact node pairs of a round: one warp per chunk. The chunk's segment
+// pairs are numbered entry by entry (entry j holds cnt1 x cnt2 of them) and
+// evaluated 32 at a time, one per lane, so a warp stays full whatever the
+// entry sizes. Sums go to the chunk's loop pair in fixed point.
+struct BucketArgs {
+  const double *xyz;
+  const int64_t *off;
+  const int32_t *slot_loops;
+  const BucketChunk *chunks;
+  const unsigned long long *count;
+  int64_t cap;
+  unsigned long long *acc_lk;
+  double *counts;  // [1] segment pairs summed exactly
+};
+
+__global__ void __launch_bounds__(256) bh_buckets(BucketArgs A) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t n = min((int64_t)*A.count, A.cap);
+  double nexact = 0;
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += nw) {
+    const int slot = A.chunks[c].slot, cnt = A.chunks[c].count;
+    const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
+    const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
+    int4 e = make_int4(0, 0, 0, 1);
+    if (lane < cnt) e = A.chunks[c].e[lane];
+    const int np = lane < cnt ? e.z * e.w : 0;
+    int incl = np;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - np;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    double sum = 0.0;
+    for (int base = 0; base < total; base += 32) {
+      const int g = base + lane;
+      // the last entry starting at or before g (entries past cnt start at total)
+      int j = 0;
+#pragma unroll
+      for (int st = 16; st; st >>= 1) {
+        const int x = __shfl_sync(0xffffffffu, excl, j + st);
+        if (x <= g) j += st;
+      }
+      const int lo1 = __shfl_sync(0xffffffffu, e.x, j), lo2 = __shfl_sync(0xffffffffu, e.y, j);
+      const int c2 = __shfl_sync(0xffffffffu, e.w, j), ex = __shfl_sync(0xffffffffu, excl, j);
+      if (g < total) {
+        const int off = g - ex, u = off / c2, v = off - u * c2;
+        seg_pair_eval(A.xyz, o1, n1, lo1 + u, o2, n2, lo2 + v, sum);
+      }
+    }
+    nexact += total;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) fix_add(A.acc_lk + slot, sum);
+  }
+  if (lane == 0 && nexact > 0) atomicAdd(A.counts + 1, nexact);
 }
 
 #ifdef FLN_BH_MIN_CTAS
@@ -1866,6 +2013,8 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
   const double b0 = prm.barnes_hut_init_beta;
   const int budget = prm.bh_budget > 0 ? prm.bh_budget : FLN_BH_BUDGET;
+  // Buckets need contiguous segment ranges: curve-order trees only.
+  const int bucket = prm.bh_tree == 1 ? 1 : (prm.bh_bucket > 0 ? prm.bh_bucket : FLN_BH_BUCKET);
   if ((ctx.learned.frag || ctx.recording.rec) && prm.bh_schedule != 0)
     throw Error(FLN_ERR_INVALID_ARGUMENT, "The learned opening criterion runs with bh_schedule 0 only.");
   // Chunk lists of the split evaluation: a warp can write at most budget + 2
@@ -1873,6 +2022,13 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   const int64_t chunk_soft = int64_t(1) << FLN_CHUNK_SOFT_LOG2;
   const int64_t chunk_cap = chunk_soft + std::max(nwarps, nwarps_c) * (budget + 2);
   Chunk *d_far = nullptr, *d_leaf = nullptr;
+  // Exact list of the fused rounds: past the soft limit a round takes no new
+  // batch; a warp writes at most budget + 2 chunks after that.
+  const int64_t bkt_soft = int64_t(1) << FLN_BUCKET_SOFT_LOG2;
+  const int64_t bkt_cap = bkt_soft + nwarps * (budget + 2);
+  BucketChunk *d_bkt = nullptr;
+  if (prm.bh_schedule == 0)
+    d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)bkt_cap * sizeof(BucketChunk)));
   if (prm.bh_schedule == 2) {
     d_far = reinterpret_cast<Chunk *>(ctx.d_bh[16].need((size_t)chunk_cap * sizeof(Chunk)));
     d_leaf = reinterpret_cast<Chunk *>(ctx.d_bh[17].need((size_t)chunk_cap * sizeof(Chunk)));
@@ -1928,8 +2084,8 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         continue;
       }
       TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
-                 d_batch[1 - cur], cap, d_ctr + 1, budget, d_acc, d_acc_err, d_counts, d_spill, d_ctr, d_status,
-                 ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
+                 d_batch[1 - cur], cap, d_ctr + 1, budget, bucket, d_bkt, d_ctr + 2, bkt_soft, bkt_cap, d_acc,
+                 d_acc_err, d_counts, d_spill, d_ctr, d_status, ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
       if (record) {
         A.rec = ctx.recording.rec;
         A.rec_count = ctx.recording.count;
@@ -1946,12 +2102,25 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       else
         bh_traverse<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
-      ++launches;
+      BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc, d_counts};
+      bh_buckets<<<ctx.num_sms * 8, 256, 0, st>>>(BA);
+      FLN_CUDA(cudaGetLastError());
+      launches += 2;
       ++ctx.stats.bh_rounds;
-      unsigned long long next = 0;
-      FLN_CUDA(cudaMemcpyAsync(&next, d_ctr + 1, sizeof next, cudaMemcpyDeviceToHost, st));
+      unsigned long long c2[2];
+      FLN_CUDA(cudaMemcpyAsync(c2, d_ctr, sizeof c2, cudaMemcpyDeviceToHost, st));
       FLN_CUDA(cudaStreamSynchronize(st));
-      nin = (int64_t)std::min<unsigned long long>(next, (unsigned long long)cap);
+      // Batches not taken this round (past the soft limit) carry over.
+      int64_t next = (int64_t)std::min<unsigned long long>(c2[1], (unsigned long long)cap);
+      const int64_t taken = (int64_t)std::min<unsigned long long>(c2[0], (unsigned long long)nin);
+      if (taken < nin) {
+        const int64_t keep = std::min<int64_t>(nin - taken, cap - next);
+        FLN_CUDA(cudaMemcpyAsync(d_batch[1 - cur] + next, d_batch[cur] + taken, keep * sizeof(Batch),
+                                 cudaMemcpyDeviceToDevice, st));
+        if (keep < nin - taken) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut round buffer too small");
+        next += keep;
+      }
+      nin = next;
       cur = 1 - cur;
     }
   };

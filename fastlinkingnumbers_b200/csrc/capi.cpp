@@ -223,6 +223,7 @@ static fln_params resolved(const fln_params *p) {
   if (r.bh_schedule < 0 || r.bh_schedule > 2) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_schedule in [0, 2]");
   if (r.bh_budget != 0 && (r.bh_budget < 16 || r.bh_budget > 4096))
     throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_budget 0 or in [16, 4096]");
+  if (r.bh_bucket < 0 || r.bh_bucket > 16) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_bucket in [0, 16]");
   return r;
 }
 

@@ -91,7 +91,10 @@ typedef struct fln_params {
   int32_t bh_budget;            /* traversal steps a warp spends on a batch per launch before handing the
                                    rest on; 0 = 256. The node pairs stay the same; only the grouping of
                                    the FP64 partial sums changes (last-bit differences). */
-  int32_t reserved[1];
+  int32_t bh_bucket;            /* curve-order trees, bh_schedule 0: a node pair that is neither far nor a
+                                   leaf pair and has at most this many segments a side is summed exactly,
+                                   segment pair by segment pair; 0 = 8, 1 = leaf pairs only (the
+                                   reference's traversal), at most 16 */
 } fln_params;
 
 /* Statistics of the last computation on a context. */

@@ -210,11 +210,12 @@ def test_traversal_schedules_agree(engine, name, golden_dir):
     # 0.1)^(1/4) beta0, is computed by the host for rounds and on the device
     # for the persistent queue; one ulp of difference can flip a node pair
     # that sits on the opening boundary, so retried pairs agree within the
-    # Barnes-Hut error and pairs run once agree to rounding.
+    # Barnes-Hut error and pairs run once agree to rounding. The persistent
+    # and split schedules sum leaf pairs only (bh_bucket 1).
     _, off, xyz, pairs = _prepared(name, golden_dir)
     runs = []
     for sched in (0, 1, 2):
-        lk, err, fl = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=sched)
+        lk, err, fl = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_schedule=sched, bh_bucket=1)
         runs.append((lk, err, fl, engine.stats()))
     lk0, err0, fl0, s0 = runs[0]
     for lk, err, fl, s in runs[1:]:
@@ -225,6 +226,56 @@ def test_traversal_schedules_agree(engine, name, golden_dir):
         assert np.array_equal(np.rint(lk), np.rint(lk0))
         np.testing.assert_allclose(lk, lk0, rtol=0, atol=0.05)
         assert s["bh_wait_timeouts"] == 0
+
+
+@pytest.mark.parametrize("name", ["knittubebroken", "glove"])
+def test_buckets_keep_integers(engine, name, golden_dir):
+    # Node pairs of at most bh_bucket segments a side are summed exactly
+    # instead of being split further: fewer far-field terms, the same
+    # integers, sums within the Barnes-Hut target error (0.1) of the FP64
+    # direct sum.
+    _, off, xyz, pairs = _prepared(name, golden_dir)
+    ref = np.load(os.path.join(GOLDEN, "pairs", name + ".npz"))
+    lk1, err1, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_bucket=1)
+    s1 = engine.stats()
+    assert np.array_equal(np.rint(lk1), np.rint(ref["lk_direct"]))
+    for b in (2, 4, 8, 16):
+        lk, err, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_bucket=b)
+        s = engine.stats()
+        assert np.array_equal(np.rint(lk), np.rint(ref["lk_direct"]))
+        np.testing.assert_allclose(lk, ref["lk_direct"], rtol=0, atol=0.1)
+        assert s["bh_far_evals"] < s1["bh_far_evals"]
+        assert s["bh_leaf_evals"] > s1["bh_leaf_evals"]
+
+
+def test_buckets_ignored_on_reference_tree(engine, golden_dir):
+    # The kd-median tree has no contiguous segment ranges: bh_bucket has no
+    # effect there (leaf pairs only, the reference's traversal).
+    _, off, xyz, pairs = _prepared("knittubebroken", golden_dir)
+    a, ea, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_tree=1, bh_bucket=1)
+    b, eb, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_tree=1, bh_bucket=16)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(ea, eb)
+
+
+def test_buckets_on_polymer_loops(engine):
+    # Long random walks, where most of the work sits near the leaves: every
+    # bucket size gives the integers of the FP64 direct sum on a sample.
+    off, xyz = workloads.polymer(seed=71, n_loops=24, n_steps=20_000, cube=220.0)
+    m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
+    poff, pxyz, pairs, _ = m.Prepare(True, engine=engine)
+    pick = np.random.default_rng(5).permutation(len(pairs))[:12]
+    lk64, _, _ = engine.linking_numbers(pxyz, poff, pairs[pick], "directsum", precision=N.PREC_FP64)
+    for b in (1, 4, 8, 16):
+        lk, err, fl = engine.linking_numbers(pxyz, poff, pairs, "barneshut", bh_bucket=b)
+        assert np.array_equal(np.rint(lk[pick]), np.rint(lk64))
+        assert np.abs(lk[pick] - lk64).max() < 0.1
+
+
+def test_bucket_argument_checked(engine, golden_dir):
+    _, off, xyz, pairs = _prepared("knittubebroken", golden_dir)
+    with pytest.raises(FlnError):
+        engine.linking_numbers(xyz, off, pairs, "barneshut", bh_bucket=17)
 
 
 def test_autotune_budget_keeps_results(engine):
