@@ -614,63 +614,125 @@ __device__ __noinline__ double seg_term_fp64(const double *xyz, int64_t p0i, int
   return kInvTwoPi * atan2(y, x) + (((s < 0) || ((s == 0) && (det < 0))) ? sg : 0.0);
 }
 
-// Exact segment-pair term in FP32 (compute_link.cpp:576-606) from the
-// midpoint separation r and the two segment vectors; false (nothing added)
-// when the segments are closer than the longer one's length, where the
-// caller evaluates the pair in FP64 from its vertices.
-__device__ __forceinline__ bool seg_term_fp32(float rx, float ry, float rz, float t1x, float t1y, float t1z,
-                                              float t2x, float t2y, float t2z, float tnmax, double &sum) {
-  const float alx = rx + 0.5f * (t1x - t2x), aly = ry + 0.5f * (t1y - t2y), alz = rz + 0.5f * (t1z - t2z);
-  const float bex = rx - 0.5f * (t2x + t1x), bey = ry - 0.5f * (t2y + t1y), bez = rz - 0.5f * (t2z + t1z);
-  const float gax = rx + 0.5f * (t2x - t1x), gay = ry + 0.5f * (t2y - t1y), gaz = rz + 0.5f * (t2z - t1z);
-  const float dex = rx + 0.5f * (t2x + t1x), dey = ry + 0.5f * (t2y + t1y), dez = rz + 0.5f * (t2z + t1z);
-  const float la = sqrtf(dot3(alx, aly, alz, alx, aly, alz)), lb = sqrtf(dot3(bex, bey, bez, bex, bey, bez));
-  const float lc = sqrtf(dot3(gax, gay, gaz, gax, gay, gaz)), ld = sqrtf(dot3(dex, dey, dez, dex, dey, dez));
-  if (fminf(fminf(la, lb), fminf(lc, ld)) < tnmax) return false;
-  const float det = rx * (t2y * t1z - t2z * t1y) + ry * (t2z * t1x - t2x * t1z) + rz * (t2x * t1y - t2y * t1x);
-  const float ac = dot3(alx, aly, alz, gax, gay, gaz);
-  const float div1 = la * lb * lc + dot3(alx, aly, alz, bex, bey, bez) * lc + ac * lb + dot3(bex, bey, bez, gax, gay, gaz) * la;
-  const float div2 = la * ld * lc + dot3(alx, aly, alz, dex, dey, dez) * lc + ac * ld + dot3(dex, dey, dez, gax, gay, gaz) * la;
-  const float x = div1 * div2 - det * det;
-  const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
-  const float y = det * s;
-  const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
-  sum += kInvTwoPi * (double)atan2f(y, x) + (((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? (double)sg : 0.0);
-  return true;
+// Exact segment-pair terms in FP32, in the vertex form of the reference's
+// direct sum (compute_link.cpp:126-178): for segment p0 -> p1 of loop 1 and
+// q0 -> q1 of loop 2, a = q0 - p0, b = q0 - p1, c = q1 - p1, d = q1 - p0,
+// e = p1 - p0, f = q1 - q0, and
+//   det  = a . (f x e)
+//   div1 = |a||b||c| + (a.b)|c| + (c.a)|b| + (c.b)|a|
+//   div2 = |a||d||c| + (a.d)|c| + (c.a)|d| + (c.d)|a|
+//   term = atan2(det (div1 + div2), div1 div2 - det^2) / 2pi (+ the branch turn).
+// a, d, e and f are FP64 differences rounded once; b = a - e and c = d - e in
+// FP32. Walking q along loop 2 for a fixed p, step k+1's a, b are step k's
+// d, c, so a step forms two new vectors and two norms. Segments closer than
+// the longer one's length (squared norms compared) are left to FP64.
+
+// arctan(t) for |t| <= 1/4 from its Maclaurin series t - t^3/3 + t^5/5 - t^7/7
+// + t^9/9; the first omitted term is below 2.2e-8 |t|, under FP32 rounding.
+__device__ __forceinline__ float atan_quarter(float t) {
+  const float u = t * t;
+  float p = fmaf(u, 1.0f / 9.0f, -1.0f / 7.0f);
+  p = fmaf(p, u, 1.0f / 5.0f);
+  p = fmaf(p, u, -1.0f / 3.0f);
+  p = fmaf(p, u, 1.0f);
+  return p * t;
 }
 
-// Exact leaf-leaf term from the two leaf records (midpoints, tangents); the
-// same value as seg_pair_eval of the two segments.
-__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &m1,
-                          const NodeMom &m2, int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
-  const float rx = (float)(h2.m[0] - h1.m[0]), ry = (float)(h2.m[1] - h1.m[1]), rz = (float)(h2.m[2] - h1.m[2]);
-  // The near test of seg_pair_eval, from the same FP32 segment vectors.
-  const float tn = sqrtf(fmaxf(dot3(m1.t[0], m1.t[1], m1.t[2], m1.t[0], m1.t[1], m1.t[2]),
-                               dot3(m2.t[0], m2.t[1], m2.t[2], m2.t[0], m2.t[1], m2.t[2])));
-  if (seg_term_fp32(rx, ry, rz, m1.t[0], m1.t[1], m1.t[2], m2.t[0], m2.t[1], m2.t[2], tn, sum)) return;
-  const int64_t s1 = -1 - h1.left, s2 = -1 - h2.left;
-  sum += seg_term_fp64(xyz, o1 + s1, o1 + (s1 + 1 == n1 ? 0 : s1 + 1), o2 + s2, o2 + (s2 + 1 == n2 ? 0 : s2 + 1));
+struct SegWalk {        // the carried state of a walk along loop 2
+  float ax, ay, az;     // a = q_k - p0
+  float bx, by, bz;     // b = q_k - p1
+  float aa, bb, ab;     // |a|^2, |b|^2, a.b
+  float la, lb;         // |a|, |b| (meaningful when aa, bb > 0)
+};
+
+__device__ __forceinline__ float norm_of(float sq) { return sq * rsqrtf(sq); }
+
+// The walk's first vertex q0 (FP64) for segment p0 -> p1 (e = p1 - p0, FP32).
+__device__ __forceinline__ SegWalk walk_start(const double *p0, const double *q0, float ex, float ey, float ez) {
+  SegWalk w;
+  w.ax = (float)(q0[0] - p0[0]);
+  w.ay = (float)(q0[1] - p0[1]);
+  w.az = (float)(q0[2] - p0[2]);
+  w.bx = w.ax - ex;
+  w.by = w.ay - ey;
+  w.bz = w.az - ez;
+  w.aa = dot3(w.ax, w.ay, w.az, w.ax, w.ay, w.az);
+  w.bb = dot3(w.bx, w.by, w.bz, w.bx, w.by, w.bz);
+  w.ab = dot3(w.ax, w.ay, w.az, w.bx, w.by, w.bz);
+  w.la = norm_of(w.aa);
+  w.lb = norm_of(w.bb);
+  return w;
 }
 
-// Exact term of segment s1 of loop 1 and segment s2 of loop 2 from their
-// vertices: midpoints and segment vectors in FP64 as the leaf records form
-// them (halving is exact, so the midpoint rounds once either way), the term
-// in FP32 (FP64 for close segments).
-__device__ __forceinline__ void seg_pair_eval(const double *xyz, int64_t o1, int64_t n1, int32_t s1, int64_t o2,
-                                              int64_t n2, int32_t s2, double &sum) {
+// One step q0 -> q1 of the walk: adds the term to acc (radians) and turns
+// (whole turns of the branch correction) and returns true, or returns false when the pair is near (FP64 needed). The
+// walk advances to q1 either way.
+__device__ __forceinline__ bool walk_step(SegWalk &w, const double *p0, const double *q0, const double *q1,
+                                          float ex, float ey, float ez, float ee, float &acc, float &turns) {
+  const float dx = (float)(q1[0] - p0[0]), dy = (float)(q1[1] - p0[1]), dz = (float)(q1[2] - p0[2]);
+  const float fx = (float)(q1[0] - q0[0]), fy = (float)(q1[1] - q0[1]), fz = (float)(q1[2] - q0[2]);
+  const float cx = dx - ex, cy = dy - ey, cz = dz - ez;
+  const float cc = dot3(cx, cy, cz, cx, cy, cz), dd = dot3(dx, dy, dz, dx, dy, dz);
+  const float cd = dot3(cx, cy, cz, dx, dy, dz), ff = dot3(fx, fy, fz, fx, fy, fz);
+  const float lc = norm_of(cc), ld = norm_of(dd);
+  const bool near = fminf(fminf(w.aa, w.bb), fminf(cc, dd)) <= fmaxf(ee, ff);
+  if (!near) {
+    const float ca = dot3(cx, cy, cz, w.ax, w.ay, w.az), cb = dot3(cx, cy, cz, w.bx, w.by, w.bz);
+    const float ad = dot3(w.ax, w.ay, w.az, dx, dy, dz);
+    const float det = w.ax * (fy * ez - fz * ey) + w.ay * (fz * ex - fx * ez) + w.az * (fx * ey - fy * ex);
+    const float t = w.la * lc;
+    const float div1 = t * w.lb + w.ab * lc + ca * w.lb + cb * w.la;
+    const float div2 = t * ld + ad * lc + ca * ld + cd * w.la;
+    const float x = div1 * div2 - det * det;
+    const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
+    const float y = det * s;
+    float term;
+    if (s > 0.f && fabsf(y) < 0.25f * x) {
+      term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
+    } else {
+      term = atan2f(y, x);
+      const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
+      if ((s < 0.f) || ((s == 0.f) && (det < 0.f))) turns += sg;
+    }
+    acc += term;
+  }
+  w.ax = dx; w.ay = dy; w.az = dz;
+  w.bx = cx; w.by = cy; w.bz = cz;
+  w.aa = dd; w.bb = cc; w.ab = cd;
+  w.la = ld; w.lb = lc;
+  return !near;
+}
+
+__device__ __forceinline__ void load3(const double *xyz, int64_t v, double *p) {
+  p[0] = xyz[3 * v];
+  p[1] = xyz[3 * v + 1];
+  p[2] = xyz[3 * v + 2];
+}
+
+// Exact term of segment s1 of loop 1 (vertex offset o1, n1 segments) and
+// segment s2 of loop 2: the first step of a walk, FP64 for near segments.
+__device__ __forceinline__ double seg_pair_term(const double *xyz, int64_t o1, int64_t n1, int64_t s1, int64_t o2,
+                                                int64_t n2, int64_t s2) {
   const int64_t a0 = o1 + s1, a1 = o1 + (s1 + 1 == n1 ? 0 : s1 + 1);
   const int64_t b0 = o2 + s2, b1 = o2 + (s2 + 1 == n2 ? 0 : s2 + 1);
-  float r[3], t1[3], t2[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const double p0 = xyz[3 * a0 + a], p1 = xyz[3 * a1 + a], q0 = xyz[3 * b0 + a], q1 = xyz[3 * b1 + a];
-    r[a] = (float)((0.5 * q0 + 0.5 * q1) - (0.5 * p0 + 0.5 * p1));
-    t1[a] = (float)(p1 - p0);
-    t2[a] = (float)(q1 - q0);
-  }
-  const float tn = sqrtf(fmaxf(dot3(t1[0], t1[1], t1[2], t1[0], t1[1], t1[2]), dot3(t2[0], t2[1], t2[2], t2[0], t2[1], t2[2])));
-  if (seg_term_fp32(r[0], r[1], r[2], t1[0], t1[1], t1[2], t2[0], t2[1], t2[2], tn, sum)) return;
-  sum += seg_term_fp64(xyz, a0, a1, b0, b1);
+  double p0[3], p1[3], q0[3], q1[3];
+  load3(xyz, a0, p0);
+  load3(xyz, a1, p1);
+  load3(xyz, b0, q0);
+  load3(xyz, b1, q1);
+  const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
+  SegWalk w = walk_start(p0, q0, ex, ey, ez);
+  float acc = 0.f, turns = 0.f;
+  if (walk_step(w, p0, q0, q1, ex, ey, ez, dot3(ex, ey, ez, ex, ey, ez), acc, turns))
+    return kInvTwoPi * (double)acc + (double)turns;
+  return seg_term_fp64(xyz, a0, a1, b0, b1);
+}
+
+// Exact leaf-leaf term of the traversal schedules 1 and 2; the same value as
+// the exact-list kernel gives the pair.
+__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &, const NodeMom &,
+                          int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
+  sum += seg_pair_term(xyz, o1, n1, -1 - h1.left, o2, n2, -1 - h2.left);
 }
 
 // Traversal steps a warp takes on one batch per round before it hands the
@@ -977,10 +1039,11 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
 }
 
-// Exact node pairs of a round: one warp per chunk. The chunk's segment
-// pairs are numbered entry by entry (entry j holds cnt1 x cnt2 of them) and
-// evaluated 32 at a time, one per lane, so a warp stays full whatever the
-// entry sizes. Sums go to the chunk's loop pair in fixed point.
+// Exact node pairs of a round: one warp per chunk. Entry j of a chunk is a
+// block of cnt1 x cnt2 segment pairs; its cnt1 rows (one segment of loop 1
+// against cnt2 consecutive segments of loop 2) are numbered entry by entry
+// and walked 32 at a time, one row per lane, so a warp stays full whatever
+// the entry sizes. Sums go to the chunk's loop pair in fixed point.
 struct BucketArgs {
   const double *xyz;
   const int64_t *off;
@@ -992,7 +1055,10 @@ struct BucketArgs {
   double *counts;  // [1] segment pairs summed exactly
 };
 
-__global__ void __launch_bounds__(256) bh_buckets(BucketArgs A) {
+#ifndef FLN_BUCKET_MIN_CTAS
+#define FLN_BUCKET_MIN_CTAS 3
+#endif
+__global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArgs A) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t n = min((int64_t)*A.count, A.cap);
@@ -1003,19 +1069,20 @@ __global__ void __launch_bounds__(256) bh_buckets(BucketArgs A) {
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
     int4 e = make_int4(0, 0, 0, 1);
     if (lane < cnt) e = A.chunks[c].e[lane];
-    const int np = lane < cnt ? e.z * e.w : 0;
-    int incl = np;
+    const int nr = lane < cnt ? e.z : 0;
+    int incl = nr, pairs = nr * e.w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += y;
+      pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     }
-    const int excl = incl - np;
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - nr;
+    const int rows = __shfl_sync(0xffffffffu, incl, 31);
     double sum = 0.0;
-    for (int base = 0; base < total; base += 32) {
+    for (int base = 0; base < rows; base += 32) {
       const int g = base + lane;
-      // the last entry starting at or before g (entries past cnt start at total)
+      // the last entry starting at or before row g (entries past cnt start at rows)
       int j = 0;
 #pragma unroll
       for (int st = 16; st; st >>= 1) {
@@ -1023,13 +1090,39 @@ __global__ void __launch_bounds__(256) bh_buckets(BucketArgs A) {
         if (x <= g) j += st;
       }
       const int lo1 = __shfl_sync(0xffffffffu, e.x, j), lo2 = __shfl_sync(0xffffffffu, e.y, j);
-      const int c2 = __shfl_sync(0xffffffffu, e.w, j), ex = __shfl_sync(0xffffffffu, excl, j);
-      if (g < total) {
-        const int off = g - ex, u = off / c2, v = off - u * c2;
-        seg_pair_eval(A.xyz, o1, n1, lo1 + u, o2, n2, lo2 + v, sum);
+      const int c2 = __shfl_sync(0xffffffffu, e.w, j), ex0 = __shfl_sync(0xffffffffu, excl, j);
+      if (g < rows) {
+        const int64_t s1 = lo1 + (g - ex0);
+        const int64_t a0 = o1 + s1, a1 = o1 + (s1 + 1 == n1 ? 0 : s1 + 1);
+        double p0[3], p1[3], q0[3], q1[3];
+        load3(A.xyz, a0, p0);
+        load3(A.xyz, a1, p1);
+        const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
+        const float ee = dot3(ex, ey, ez, ex, ey, ez);
+        int64_t s2 = lo2;
+        load3(A.xyz, o2 + s2, q0);
+        SegWalk w = walk_start(p0, q0, ex, ey, ez);
+        float acc = 0.f, turns = 0.f;
+        uint32_t nearmask = 0;  // steps left to FP64, evaluated after the walk (no call inside it)
+        for (int k = 0; k < c2; ++k) {
+          const int64_t s2n = s2 + 1 == n2 ? 0 : s2 + 1;
+          load3(A.xyz, o2 + s2n, q1);
+          if (!walk_step(w, p0, q0, q1, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
+          q0[0] = q1[0];
+          q0[1] = q1[1];
+          q0[2] = q1[2];
+          s2 = s2n;
+        }
+        sum += kInvTwoPi * (double)acc + (double)turns;
+        while (nearmask) {
+          const int k = __ffs(nearmask) - 1;
+          nearmask &= nearmask - 1;
+          const int64_t t0 = (lo2 + k) % n2, t1 = (lo2 + k + 1) % n2;
+          sum += seg_term_fp64(A.xyz, a0, a1, o2 + t0, o2 + t1);
+        }
       }
     }
-    nexact += total;
+    nexact += pairs;
 #pragma unroll
     for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (lane == 0) fix_add(A.acc_lk + slot, sum);
