@@ -103,7 +103,7 @@ __device__ __forceinline__ void get16(const T *src, T &dst) {
 }
 
 // Traversal records.
-struct __align__(16) NodeHdr {
+struct __align__(32) NodeHdr {
   double m[3];      // centre (leaves: segment midpoint)
   double r;         // half the box diagonal
   double rsq;       // its square, 0.25 |diag|^2, for the reference's split rule
@@ -111,17 +111,17 @@ struct __align__(16) NodeHdr {
   int32_t right;
   int32_t lo;       // leaf: its segment; curve-order node: first segment of its range
   int32_t cnt;      // leaves below (curve-order: the range is [lo, lo + cnt))
-  int32_t pad[2];   // 64 B: a record never straddles a 128 B line
+  int32_t pad[2];   // 64 B: two 32-byte loads (load_hdr), never across a 128 B line
 };
 static_assert(sizeof(NodeHdr) == 64, "NodeHdr layout");
-struct __align__(16) NodeMom {
+struct __align__(32) NodeMom {
   float t[3];
   float D[9];
   float Q[18];
   float tn, dn, qn;
-  float pad[3];
+  float pad[7];     // 160 B: five 32-byte loads (load_mom)
 };
-static_assert(sizeof(NodeMom) == 144, "NodeMom layout");
+static_assert(sizeof(NodeMom) == 160, "NodeMom layout");
 
 struct TreeArgs {
   const double *xyz;
@@ -277,7 +277,7 @@ __device__ void finish_record_regs(const BuildNode &B, NodeHdr &H, NodeMom &M, b
   M.dn = (float)(sqrt(dd) * kInvRt3);
   // Leaf: |c|^3 / 36, which is also (1/3) ||C_Q||_F for c c c^T / 12.
   M.qn = (float)(leaf ? tn * tn * tn / 36.0 : sqrt(qq) / 3.0);
-  M.pad[0] = M.pad[1] = M.pad[2] = 0.f;
+  for (int a = 0; a < 7; ++a) M.pad[a] = 0.f;
 }
 
 // Traversal records of a node, formed in registers and stored as vectors.
@@ -783,6 +783,27 @@ __device__ __noinline__ void shift_down(int2 *stack, int k, int n, int lane) {
 // spreads over many warps while light pairs finish in one go.
 // kLearn: the learned opening criterion (A.learned); kRecord: sampling of
 // training node pairs (A.rec). The plain instantiation has neither.
+// Traversal records through the read-only path in 32-byte loads: the
+// traversal is bound by L1 wavefronts, and a scattered 32-byte load costs
+// one per lane where two 16-byte loads cost two.
+__device__ __forceinline__ void load32(const void *p, unsigned long long *w) {
+  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(w[0]), "=l"(w[1]), "=l"(w[2]), "=l"(w[3]) : "l"(p));
+}
+__device__ __forceinline__ NodeHdr load_hdr(const NodeHdr *p) {
+  NodeHdr h;
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(&h);
+  load32(p, w);
+  load32(reinterpret_cast<const char *>(p) + 32, w + 4);
+  return h;
+}
+__device__ __forceinline__ NodeMom load_mom(const NodeMom *p) {
+  NodeMom m;
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(&m);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) load32(reinterpret_cast<const char *>(p) + 32 * i, w + 4 * i);
+  return m;
+}
+
 template <bool kLearn, bool kRecord>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ int2 s_stack[kWarps][kStack];
@@ -877,7 +898,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       float sep = 0.f;
       double dsq = 0.0;
       if (act) {
-        const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+        const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
         const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
         const double rs = h1.r + h2.r;
@@ -925,7 +946,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
           float f[kMlpIn];
           for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
           if (cand) {
-            const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+            const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
             const NodeMom &ma = M1[pr.x], &mb = M2[pr.y];
             mlp_features(sep, (float)h1.r, (float)h2.r, dsq, ma.tn, mb.tn, ma.dn, mb.dn, ma.qn, mb.qn, f);
           }
@@ -1001,9 +1022,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
 #endif
       while (nf >= 32) {
         const int2 q = farq[nf - 32 + lane];
-        const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+        const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-        far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
+        far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
                  (float)h1.r, (float)h2.r, sum, err);
         nfar += 32;
         nf -= 32;
@@ -1013,9 +1034,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     // Evaluate what is still queued.
     if (lane < nf) {
       const int2 q = farq[lane];
-      const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+      const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
       const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-      far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
+      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
                (float)h2.r, sum, err);
     }
     if (bc >= 0 && lane == 0 && bc < A.bkt_cap) {
