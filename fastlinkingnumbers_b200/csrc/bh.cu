@@ -123,6 +123,30 @@ struct __align__(32) NodeMom {
 };
 static_assert(sizeof(NodeMom) == 160, "NodeMom layout");
 
+// Traversal records through the read-only path in 32-byte loads: the
+// traversal is bound by L1 wavefronts, and a scattered 32-byte load costs
+// one per lane where two 16-byte loads cost two. Every kernel that
+// classifies or evaluates node pairs loads them this way, so the compiled
+// arithmetic, and with it every rounding, is the same in all schedules.
+__device__ __forceinline__ void load32(const void *p, unsigned long long *w) {
+  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(w[0]), "=l"(w[1]), "=l"(w[2]), "=l"(w[3]) : "l"(p));
+}
+__device__ __forceinline__ NodeHdr load_hdr(const NodeHdr *p) {
+  NodeHdr h;
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(&h);
+  load32(p, w);
+  load32(reinterpret_cast<const char *>(p) + 32, w + 4);
+  return h;
+}
+__device__ __forceinline__ NodeMom load_mom(const NodeMom *p) {
+  NodeMom m;
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(&m);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) load32(reinterpret_cast<const char *>(p) + 32 * i, w + 4 * i);
+  return m;
+}
+
+
 struct TreeArgs {
   const double *xyz;
   const int64_t *off;        // loop vertex offsets
@@ -783,27 +807,6 @@ __device__ __noinline__ void shift_down(int2 *stack, int k, int n, int lane) {
 // spreads over many warps while light pairs finish in one go.
 // kLearn: the learned opening criterion (A.learned); kRecord: sampling of
 // training node pairs (A.rec). The plain instantiation has neither.
-// Traversal records through the read-only path in 32-byte loads: the
-// traversal is bound by L1 wavefronts, and a scattered 32-byte load costs
-// one per lane where two 16-byte loads cost two.
-__device__ __forceinline__ void load32(const void *p, unsigned long long *w) {
-  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(w[0]), "=l"(w[1]), "=l"(w[2]), "=l"(w[3]) : "l"(p));
-}
-__device__ __forceinline__ NodeHdr load_hdr(const NodeHdr *p) {
-  NodeHdr h;
-  unsigned long long *w = reinterpret_cast<unsigned long long *>(&h);
-  load32(p, w);
-  load32(reinterpret_cast<const char *>(p) + 32, w + 4);
-  return h;
-}
-__device__ __forceinline__ NodeMom load_mom(const NodeMom *p) {
-  NodeMom m;
-  unsigned long long *w = reinterpret_cast<unsigned long long *>(&m);
-#pragma unroll
-  for (int i = 0; i < 5; ++i) load32(reinterpret_cast<const char *>(p) + 32 * i, w + 4 * i);
-  return m;
-}
-
 template <bool kLearn, bool kRecord>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ int2 s_stack[kWarps][kStack];
@@ -1285,7 +1288,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_classify(ClassifyArgs A) {
       int kind = 0;
       int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
       if (act) {
-        const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+        const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
         const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
         const double rs = h1.r + h2.r;
@@ -1376,9 +1379,9 @@ __global__ void __launch_bounds__(256) bh_far_chunks(EvalArgs A) {
   double sum = 0.0, err = 0.0;
   if (lane < n) {
     const int2 q = A.chunks[c].pairs[lane];
-    const NodeHdr h1 = A.hdr[b1 + q.x], h2 = A.hdr[b2 + q.y];
+    const NodeHdr h1 = load_hdr(A.hdr + b1 + q.x), h2 = load_hdr(A.hdr + b2 + q.y);
     const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-    far_eval(A.mom[b1 + q.x], A.mom[b2 + q.y], (float)dx, (float)dy, (float)dz,
+    far_eval(load_mom(A.mom + b1 + q.x), load_mom(A.mom + b2 + q.y), (float)dx, (float)dy, (float)dz,
              dx * dx + dy * dy + dz * dz + A.epssq, (float)h1.r, (float)h2.r, sum, err);
   }
   for (int o = 16; o; o >>= 1) {
@@ -1709,7 +1712,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
       int kind = 0;
       int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
       if (act) {
-        const NodeHdr h1 = H1[pr.x], h2 = H2[pr.y];
+        const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
         const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
         const double rs = h1.r + h2.r;
@@ -1759,9 +1762,9 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
       __syncwarp();
       while (nf >= 32) {
         const int2 q = farq[nf - 32 + lane];
-        const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+        const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-        far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
+        far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
                  (float)h1.r, (float)h2.r, sum, err);
         nfar += 32;
         nf -= 32;
@@ -1777,9 +1780,9 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
     }
     if (lane < nf) {
       const int2 q = farq[lane];
-      const NodeHdr h1 = H1[q.x], h2 = H2[q.y];
+      const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
       const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-      far_eval(M1[q.x], M2[q.y], (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
+      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
                (float)h2.r, sum, err);
     }
     if (lane < nl) {
@@ -1824,8 +1827,8 @@ __global__ void sample_features(const int64_t *node_base, const NodeHdr *hdr, co
   const int4 sm = samples[k];
   const int l1 = slot_loops[2 * sm.x], l2 = slot_loops[2 * sm.x + 1];
   const int64_t b1 = node_base[l1], b2 = node_base[l2];
-  const NodeHdr h1 = hdr[b1 + sm.y], h2 = hdr[b2 + sm.z];
-  const NodeMom &m1 = mom[b1 + sm.y], &m2 = mom[b2 + sm.z];
+  const NodeHdr h1 = load_hdr(hdr + b1 + sm.y), h2 = load_hdr(hdr + b2 + sm.z);
+  const NodeMom m1 = load_mom(mom + b1 + sm.y), m2 = load_mom(mom + b2 + sm.z);
   const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
   const double dsq = dx * dx + dy * dy + dz * dz + epssq;
   const float sep = (float)(sqrt(dsq) / (h1.r + h2.r));
