@@ -1064,10 +1064,18 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
 }
 
 // Exact node pairs of a round: one warp per chunk. Entry j of a chunk is a
-// block of cnt1 x cnt2 segment pairs; its cnt1 rows (one segment of loop 1
-// against cnt2 consecutive segments of loop 2) are numbered entry by entry
-// and walked 32 at a time, one row per lane, so a warp stays full whatever
-// the entry sizes. Sums go to the chunk's loop pair in fixed point.
+// block of cnt1 x cnt2 segment pairs, cut into runs of up to kRun
+// consecutive segments of loop 2 against one segment of loop 1. The runs are
+// numbered entry by entry and walked 32 at a time, one run per lane, so a
+// warp stays full whatever the entry sizes. Segment pairs left to FP64 (a
+// few percent) wait in a per-warp queue and are evaluated 32 at a time, so
+// that path runs with full warps too. Sums go to the chunk's loop pair in
+// fixed point.
+#ifndef FLN_BUCKET_RUN
+#define FLN_BUCKET_RUN 4
+#endif
+constexpr int kRun = FLN_BUCKET_RUN;
+
 struct BucketArgs {
   const double *xyz;
   const int64_t *off;
@@ -1083,7 +1091,9 @@ struct BucketArgs {
 #define FLN_BUCKET_MIN_CTAS 3
 #endif
 __global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArgs A) {
+  __shared__ int2 s_near[8][64];  // (segment of loop 1, segment of loop 2) per warp
   const int lane = threadIdx.x & 31;
+  int2 *nq = s_near[threadIdx.x >> 5];
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t n = min((int64_t)*A.count, A.cap);
   double nexact = 0;
@@ -1093,20 +1103,23 @@ __global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArg
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
     int4 e = make_int4(0, 0, 0, 1);
     if (lane < cnt) e = A.chunks[c].e[lane];
-    const int nr = lane < cnt ? e.z : 0;
-    int incl = nr, pairs = nr * e.w;
+    const int nruns = (e.w + kRun - 1) / kRun;   // runs per row
+    const int ni = lane < cnt ? e.z * nruns : 0;  // runs of the entry
+    int incl = ni, pairs = lane < cnt ? e.z * e.w : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += y;
       pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     }
-    const int excl = incl - nr;
-    const int rows = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - ni;
+    const int items = __shfl_sync(0xffffffffu, incl, 31);
+    const double *P1 = A.xyz + 3 * o1, *Q2 = A.xyz + 3 * o2;
     double sum = 0.0;
-    for (int base = 0; base < rows; base += 32) {
+    int nn = 0;  // queued FP64 pairs
+    for (int base = 0; base < items; base += 32) {
       const int g = base + lane;
-      // the last entry starting at or before row g (entries past cnt start at rows)
+      // the last entry starting at or before run g (entries past cnt start at items)
       int j = 0;
 #pragma unroll
       for (int st = 16; st; st >>= 1) {
@@ -1115,37 +1128,62 @@ __global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArg
       }
       const int lo1 = __shfl_sync(0xffffffffu, e.x, j), lo2 = __shfl_sync(0xffffffffu, e.y, j);
       const int c2 = __shfl_sync(0xffffffffu, e.w, j), ex0 = __shfl_sync(0xffffffffu, excl, j);
-      if (g < rows) {
-        const int64_t s1 = lo1 + (g - ex0);
-        const int64_t a0 = o1 + s1, a1 = o1 + (s1 + 1 == n1 ? 0 : s1 + 1);
+      const int nr = __shfl_sync(0xffffffffu, nruns, j);
+      uint32_t nearmask = 0;  // steps of this lane's run left to FP64
+      int s1 = 0, s2 = 0;
+      if (g < items) {
+        const int off = g - ex0, u = off / nr, r = off - u * nr;
+        const int v0 = r * kRun, m = min(kRun, c2 - v0);
+        s1 = lo1 + u;
+        const int s1n = s1 + 1 == n1 ? 0 : s1 + 1;
         double p0[3], p1[3], q0[3], q1[3];
-        load3(A.xyz, a0, p0);
-        load3(A.xyz, a1, p1);
+        load3(P1, s1, p0);
+        load3(P1, s1n, p1);
         const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
         const float ee = dot3(ex, ey, ez, ex, ey, ez);
-        int64_t s2 = lo2;
-        load3(A.xyz, o2 + s2, q0);
+        s2 = lo2 + v0;
+        load3(Q2, s2, q0);
         SegWalk w = walk_start(p0, q0, ex, ey, ez);
         float acc = 0.f, turns = 0.f;
-        uint32_t nearmask = 0;  // steps left to FP64, evaluated after the walk (no call inside it)
-        for (int k = 0; k < c2; ++k) {
-          const int64_t s2n = s2 + 1 == n2 ? 0 : s2 + 1;
-          load3(A.xyz, o2 + s2n, q1);
-          if (!walk_step(w, p0, q0, q1, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
-          q0[0] = q1[0];
-          q0[1] = q1[1];
-          q0[2] = q1[2];
-          s2 = s2n;
+#pragma unroll
+        for (int k = 0; k < kRun; ++k) {
+          if (k < m) {
+            const int t = s2 + k + 1;
+            load3(Q2, t == n2 ? 0 : t, q1);
+            if (!walk_step(w, p0, q0, q1, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
+            q0[0] = q1[0];
+            q0[1] = q1[1];
+            q0[2] = q1[2];
+          }
         }
         sum += kInvTwoPi * (double)acc + (double)turns;
-        while (nearmask) {
+      }
+      // Queue this pass's FP64 pairs, one per lane per round; evaluate 32 at a time.
+      while (__any_sync(0xffffffffu, nearmask != 0)) {
+        const bool has = nearmask != 0;
+        const unsigned bm = __ballot_sync(0xffffffffu, has);
+        if (has) {
           const int k = __ffs(nearmask) - 1;
           nearmask &= nearmask - 1;
-          const int64_t t0 = (lo2 + k) % n2, t1 = (lo2 + k + 1) % n2;
-          sum += seg_term_fp64(A.xyz, a0, a1, o2 + t0, o2 + t1);
+          nq[nn + __popc(bm & ((1u << lane) - 1))] = make_int2(s1, s2 + k);
+        }
+        nn += __popc(bm);
+        __syncwarp();
+        if (nn >= 32) {
+          const int2 q = nq[nn - 32 + lane];
+          sum += seg_term_fp64(A.xyz, o1 + q.x, o1 + (q.x + 1 == n1 ? 0 : q.x + 1), o2 + q.y,
+                               o2 + (q.y + 1 == n2 ? 0 : q.y + 1));
+          nn -= 32;
+          __syncwarp();
         }
       }
     }
+    if (lane < nn) {
+      const int2 q = nq[lane];
+      sum += seg_term_fp64(A.xyz, o1 + q.x, o1 + (q.x + 1 == n1 ? 0 : q.x + 1), o2 + q.y,
+                           o2 + (q.y + 1 == n2 ? 0 : q.y + 1));
+    }
+    __syncwarp();
     nexact += pairs;
 #pragma unroll
     for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
