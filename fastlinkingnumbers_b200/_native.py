@@ -80,6 +80,7 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int32), ("ms_main_kernel", C.c_double),
         ("ms_tree_build", C.c_double), ("bh_rounds", C.c_int32), ("reserved_stats", C.c_int32),
         ("bh_escalated", C.c_int64), ("bh_wait_timeouts", C.c_int64),
+        ("ms_exact", C.c_double), ("bh_exact_entries", C.c_double),
     ]
 
     def as_dict(self):

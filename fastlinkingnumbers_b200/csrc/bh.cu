@@ -823,7 +823,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     __syncthreads();
   }
   int2 *spill = A.spill + (size_t)gw * kSpill;
-  double nfar = 0;
+  double nfar = 0, nent = 0;
   for (;;) {
     long long b = 0;
     if (lane == 0) {
@@ -990,6 +990,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       nf += __popc(fm);
       if (lm) {  // append the exact pairs to the list, 32 entries per chunk
         const int ne = __popc(lm), pos = bfill + __popc(lm & ((1u << lane) - 1));
+        nent += ne;
         const int need = (bc < 0 ? 1 : 0) + (bfill + ne > 32 ? 1 : 0);
         long long c = 0;
         if (lane == 0 && need) c = (long long)atomicAdd(A.bkt_count, (unsigned long long)need);
@@ -1060,6 +1061,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
   if (lane == 0) {
     atomicAdd(A.counts, nfar);
+    atomicAdd(A.counts + 5, nent);
   }
 }
 
@@ -2166,6 +2168,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_slots, slot_loops.data(), 2 * np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_slot_pair, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
+  FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
   const double b0 = prm.barnes_hut_init_beta;
   const int budget = prm.bh_budget > 0 ? prm.bh_budget : FLN_BH_BUDGET;
   // Buckets need contiguous segment ranges: curve-order trees only.
@@ -2258,13 +2261,16 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         bh_traverse<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
       BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc, d_counts};
+      FLN_CUDA(cudaEventRecord(ctx.ev_bk[0], st));
       bh_buckets<<<ctx.num_sms * 8, 256, 0, st>>>(BA);
       FLN_CUDA(cudaGetLastError());
+      FLN_CUDA(cudaEventRecord(ctx.ev_bk[1], st));
       launches += 2;
       ++ctx.stats.bh_rounds;
       unsigned long long c2[2];
       FLN_CUDA(cudaMemcpyAsync(c2, d_ctr, sizeof c2, cudaMemcpyDeviceToHost, st));
       FLN_CUDA(cudaStreamSynchronize(st));
+      ctx.stats.ms_exact += ctx.elapsed(ctx.ev_bk[0], ctx.ev_bk[1]);
       // Batches not taken this round (past the soft limit) carry over.
       int64_t next = (int64_t)std::min<unsigned long long>(c2[1], (unsigned long long)cap);
       const int64_t taken = (int64_t)std::min<unsigned long long>(c2[0], (unsigned long long)nin);
@@ -2338,6 +2344,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     ctx.stats.bh_wait_timeouts += 1;
     d_status = reinterpret_cast<int32_t *>(d_counts + 2);
     FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
+  FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
   }
   std::vector<int32_t> all(np);
   std::iota(all.begin(), all.end(), 0);
@@ -2370,7 +2377,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     }
   }
   ctx.stats.beta_retried = (int64_t)retry_slots.size();
-  std::vector<double> far_leaf(2, 0.0);
+  std::vector<double> far_leaf(6, 0.0);
   if (!retry_slots.empty()) {
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
     pass(retry_slots, itol, false);
@@ -2420,12 +2427,13 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
     for (int32_t s : up) err[order[s]] = e3[order[s]] * prm.error_est_scale;
   }
-  FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
   FLN_CUDA(cudaMemcpyAsync(d_err_out, err.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
   if (d_flags_out) FLN_CUDA(cudaMemcpyAsync(d_flags_out, flags.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaStreamSynchronize(st));
   ctx.stats.bh_far_evals = far_leaf[0];
   ctx.stats.bh_leaf_evals = far_leaf[1];
+  ctx.stats.bh_exact_entries = prm.bh_schedule == 0 ? far_leaf[5] : far_leaf[1];
   if (status != 0)
     throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
                                             std::to_string(maxdepth) + ").");

@@ -31,6 +31,7 @@ Context::Context(int dev, void *user_stream) : device(dev) {
   FLN_CUDA(cudaEventCreate(&ev1));
   FLN_CUDA(cudaEventCreate(&ev2));
   FLN_CUDA(cudaEventCreate(&ev3));
+  for (cudaEvent_t &e : ev_bk) FLN_CUDA(cudaEventCreate(&e));
 }
 
 Context::~Context() {
@@ -48,6 +49,8 @@ Context::~Context() {
   if (ev2) cudaEventDestroy(ev2);
   if (ev3) cudaEventDestroy(ev3);
   for (cudaEvent_t e : ev_stage)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ev_bk)
     if (e) cudaEventDestroy(e);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }

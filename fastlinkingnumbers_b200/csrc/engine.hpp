@@ -106,6 +106,7 @@ struct Context {
   DevBuf d_bh[24];
   HostBuf h_in, h_out;  // pinned staging of copy_h2d / copy_d2h
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev_bk[2] = {nullptr, nullptr};  // around each exact-list launch
   // Learned criterion in use on this context, and training buffers.
   DevBuf d_mlp, d_learn[8];
   // Device Discretize (discretize.cu).

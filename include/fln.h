@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define FLN_ABI_VERSION 1
+#define FLN_ABI_VERSION 2
 
 typedef enum fln_status {
   FLN_OK = 0,
@@ -119,6 +119,9 @@ typedef struct fln_stats {
   int32_t reserved_stats;
   int64_t bh_escalated;         /* pair re-runs with an escalated beta */
   int64_t bh_wait_timeouts;     /* persistent traversals that fell back to rounds */
+  double ms_exact;              /* Barnes–Hut: device time of the exact-list kernel (part of ms_main_kernel) */
+  double bh_exact_entries;      /* Barnes–Hut: node pairs summed exactly (leaf pairs and small node pairs);
+                                   bh_leaf_evals counts their segment pairs */
 } fln_stats;
 
 typedef struct fln_ctx fln_ctx;
