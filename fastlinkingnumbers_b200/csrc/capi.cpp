@@ -141,6 +141,7 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   ctx.stats.ms_main_kernel = 0;
   ctx.stats.ms_tree_build = 0;
   ctx.stats.bh_far_evals = ctx.stats.bh_leaf_evals = 0;
+  ctx.stats.ms_exact = ctx.stats.bh_exact_entries = 0;
   ctx.stats.beta_retried = 0;
   ctx.stats.bh_escalated = 0;
   if (!d_err) d_err = ctx.d_err.as<double>(std::max<int64_t>(np, 1));  // Barnes–Hut needs one
