@@ -60,9 +60,10 @@ constexpr int kWarps = 4;          // warps per traversal CTA
 #ifndef FLN_BH_STACK
 #define FLN_BH_STACK 224
 #endif
-// Preferred shared-memory carveout of the traversal kernel, percent.
+// Preferred shared-memory carveout of the traversal kernel, percent: room
+// for five CTAs of 15 KB (stacks, far-pair queue with its separations).
 #ifndef FLN_BH_CARVEOUT
-#define FLN_BH_CARVEOUT 28
+#define FLN_BH_CARVEOUT 44
 #endif
 constexpr int kStack = FLN_BH_STACK;
 constexpr int kSpill = 8192;       // global spill entries per warp
@@ -646,8 +647,9 @@ __device__ __noinline__ double seg_term_fp64(const double *xyz, int64_t p0i, int
 //   div1 = |a||b||c| + (a.b)|c| + (c.a)|b| + (c.b)|a|
 //   div2 = |a||d||c| + (a.d)|c| + (c.a)|d| + (c.d)|a|
 //   term = atan2(det (div1 + div2), div1 div2 - det^2) / 2pi (+ the branch turn).
-// a, d, e and f are FP64 differences rounded once; b = a - e and c = d - e in
-// FP32. Walking q along loop 2 for a fixed p, step k+1's a, b are step k's
+// a, d and e are FP64 differences rounded once; b = a - e, c = d - e and
+// f = d - a in FP32 (f's rounding, about one unit in the last place of |d|,
+// enters the term scaled by 1/|d|^2). Walking q along loop 2 for a fixed p, step k+1's a, b are step k's
 // d, c, so a step forms two new vectors and two norms. Segments closer than
 // the longer one's length (squared norms compared) are left to FP64.
 
@@ -691,10 +693,10 @@ __device__ __forceinline__ SegWalk walk_start(const double *p0, const double *q0
 // One step q0 -> q1 of the walk: adds the term to acc (radians) and turns
 // (whole turns of the branch correction) and returns true, or returns false when the pair is near (FP64 needed). The
 // walk advances to q1 either way.
-__device__ __forceinline__ bool walk_step(SegWalk &w, const double *p0, const double *q0, const double *q1,
-                                          float ex, float ey, float ez, float ee, float &acc, float &turns) {
+__device__ __forceinline__ bool walk_step(SegWalk &w, const double *p0, const double *q1, float ex, float ey,
+                                          float ez, float ee, float &acc, float &turns) {
   const float dx = (float)(q1[0] - p0[0]), dy = (float)(q1[1] - p0[1]), dz = (float)(q1[2] - p0[2]);
-  const float fx = (float)(q1[0] - q0[0]), fy = (float)(q1[1] - q0[1]), fz = (float)(q1[2] - q0[2]);
+  const float fx = dx - w.ax, fy = dy - w.ay, fz = dz - w.az;
   const float cx = dx - ex, cy = dy - ey, cz = dz - ez;
   const float cc = dot3(cx, cy, cz, cx, cy, cz), dd = dot3(dx, dy, dz, dx, dy, dz);
   const float cd = dot3(cx, cy, cz, dx, dy, dz), ff = dot3(fx, fy, fz, fx, fy, fz);
@@ -747,7 +749,7 @@ __device__ __forceinline__ double seg_pair_term(const double *xyz, int64_t o1, i
   const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
   SegWalk w = walk_start(p0, q0, ex, ey, ez);
   float acc = 0.f, turns = 0.f;
-  if (walk_step(w, p0, q0, q1, ex, ey, ez, dot3(ex, ey, ez, ex, ey, ez), acc, turns))
+  if (walk_step(w, p0, q1, ex, ey, ez, dot3(ex, ey, ez, ex, ey, ez), acc, turns))
     return kInvTwoPi * (double)acc + (double)turns;
   return seg_term_fp64(xyz, a0, a1, b0, b1);
 }
@@ -811,11 +813,15 @@ template <bool kLearn, bool kRecord>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
+  __shared__ float4 s_farv[kWarps][64];  // separation (x, y, z) and its square, per queued far pair
+  __shared__ float2 s_farr[kWarps][64];  // the two radii
   __shared__ std::conditional_t<kLearn, MlpFrag, int> s_mlp;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + w;
   int2 *stack = s_stack[w];
   int2 *farq = s_far[w];
+  float4 *farv = s_farv[w];
+  float2 *farr = s_farr[w];
   if constexpr (kLearn) {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(A.learned.frag);
     uint32_t *dst = reinterpret_cast<uint32_t *>(&s_mlp);
@@ -900,12 +906,16 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
       float sep = 0.f;
       double dsq = 0.0;
+      float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
+      float2 fr = make_float2(0.f, 0.f);
       if (act) {
         const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
         const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
         const double rs = h1.r + h2.r;
         dsq = dx * dx + dy * dy + dz * dz + eps;
+        fv = make_float4((float)dx, (float)dy, (float)dz, (float)dsq);
+        fr = make_float2((float)h1.r, (float)h2.r);
         sep = (float)(sqrt(dsq) / rs);
         if (leaf1 && leaf2) {
           kind = 1;
@@ -980,7 +990,12 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       top += 2 * ns;
       const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
       const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
-      if (kind == 2) farq[nf + __popc(fm & ((1u << lane) - 1))] = pr;
+      if (kind == 2) {
+        const int at = nf + __popc(fm & ((1u << lane) - 1));
+        farq[at] = pr;
+        farv[at] = fv;
+        farr[at] = fr;
+      }
 #if FLN_BH_PREFETCH & 2
       if (kind == 2) {
         prefetch_record(M1 + pr.x);
@@ -1026,10 +1041,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
 #endif
       while (nf >= 32) {
         const int2 q = farq[nf - 32 + lane];
-        const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
-        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-        far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
-                 (float)h1.r, (float)h2.r, sum, err);
+        const float4 v = farv[nf - 32 + lane];
+        const float2 rr = farr[nf - 32 + lane];
+        far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)v.w, rr.x, rr.y, sum, err);
         nfar += 32;
         nf -= 32;
         __syncwarp();
@@ -1038,10 +1052,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     // Evaluate what is still queued.
     if (lane < nf) {
       const int2 q = farq[lane];
-      const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
-      const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
-               (float)h2.r, sum, err);
+      const float4 v = farv[lane];
+      const float2 rr = farr[lane];
+      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)v.w, rr.x, rr.y, sum, err);
     }
     if (bc >= 0 && lane == 0 && bc < A.bkt_cap) {
       A.bkt[bc].slot = slot;
@@ -1152,10 +1165,7 @@ __global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArg
           if (k < m) {
             const int t = s2 + k + 1;
             load3(Q2, t == n2 ? 0 : t, q1);
-            if (!walk_step(w, p0, q0, q1, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
-            q0[0] = q1[0];
-            q0[1] = q1[1];
-            q0[2] = q1[2];
+            if (!walk_step(w, p0, q1, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
           }
         }
         sum += kInvTwoPi * (double)acc + (double)turns;
