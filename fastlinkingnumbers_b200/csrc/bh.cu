@@ -2354,7 +2354,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     ctx.stats.bh_wait_timeouts += 1;
     d_status = reinterpret_cast<int32_t *>(d_counts + 2);
     FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
-  FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
+    FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
   }
   std::vector<int32_t> all(np);
   std::iota(all.begin(), all.end(), 0);
