@@ -67,6 +67,12 @@ constexpr int kWarps = 4;          // warps per traversal CTA
 #endif
 constexpr int kStack = FLN_BH_STACK;
 constexpr int kSpill = 8192;       // global spill entries per warp
+// Curve-order nodes of at most 2^kSmallHeight segments are built straight
+// from their segments (build_small), the rest level by level (build_height).
+#ifndef FLN_BUILD_SMALL_HEIGHT
+#define FLN_BUILD_SMALL_HEIGHT 4
+#endif
+constexpr int kSmallHeight = FLN_BUILD_SMALL_HEIGHT;
 #ifndef FLN_BUCKET_SOFT_LOG2
 #define FLN_BUCKET_SOFT_LOG2 19  // exact-list chunks per round before it stops taking batches
 #endif
@@ -193,7 +199,7 @@ __device__ __forceinline__ int32_t add_one_rank(int32_t *count, int32_t key, boo
 // != nullptr it also records the node's height ceil(log2(range size)) (the
 // children of a node are always lower) and counts the nodes per height.
 __global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t total_internal, uint8_t *height,
-                                    int32_t *height_count) {
+                                    int32_t *height_count, int2 *range) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (height) {  // every lane of the warp takes part in the counting
     int32_t h = 0;
@@ -221,14 +227,19 @@ __global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_
   const int32_t node = (int32_t)(g - seg_start[k]);  // local internal id
   const int64_t s = node + 1;                        // split position
   const int64_t base = A.node_base[l];
-  int64_t lo = 0, hi = n;
+  int64_t lo = 0, hi = n, psize = 0;
   int32_t par = -1;
   for (int depth = 0; depth < 64; ++depth) {
     const int64_t m = lo + (hi - lo) / 2;
     if (m == s) break;
     par = (int32_t)(m - 1);
+    psize = hi - lo;
     if (s < m) hi = m;
     else lo = m;
+  }
+  if (range) {  // the node's segment range; bit 31 of .y: its parent is built by build_height
+    const bool need = par >= 0 && psize > (int64_t(1) << kSmallHeight);
+    range[g] = make_int2((int32_t)lo, (int32_t)hi | (need ? INT_MIN : 0));
   }
   const int32_t leaf0 = (int32_t)(n - 1);
   const int32_t left = (s - lo == 1) ? leaf0 + (int32_t)lo : (int32_t)(lo + (s - lo) / 2 - 1);
@@ -399,6 +410,72 @@ __global__ void bucket_heights(const uint8_t *height, int64_t total_internal, co
   const int32_t h = g < total_internal ? height[g] : 0;
   const int32_t r = add_one_rank(cursor, h, g < total_internal);
   if (g < total_internal) bucket[height_off[h] + r] = (int32_t)g;
+}
+
+// Nodes of height 1..kSmallHeight (at most 2^kSmallHeight segments), one
+// thread each, built straight from their segments: box = the range's
+// vertices; c_M, C_D and C_Q = the leaves' moments shifted to the node centre
+// (for a leaf, C_D = 0 and C_Q,k = c_k c c^T / 12, so the shift adds c r^T and
+// c_k r r^T with r = leaf midpoint - node centre). Algebraically the pairwise
+// build of build_height; it writes no build record except for nodes whose
+// parent build_height builds. Most internal nodes are this low, so this
+// skips most of the 320-byte build records.
+__global__ void build_small(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count,
+                            const int2 *range) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const int64_t g = bucket[e];
+  const int k = find_loop_of(seg_start, A.nloops, g);
+  const int l = A.loops[k];
+  const int64_t o = A.off[l], n = A.off[l + 1] - o;
+  const int64_t base = A.node_base[l];
+  const int32_t node = (int32_t)(g - seg_start[k]);
+  const int2 rg = range[g];
+  const int32_t lo = rg.x, hi = rg.y & INT_MAX;
+  const bool need = rg.y < 0;
+  const double *V = A.xyz + 3 * o;
+  BuildNode P;
+  for (int a = 0; a < 3; ++a) {
+    P.lo[a] = V[3 * lo + a];
+    P.hi[a] = P.lo[a];
+  }
+  for (int32_t v = lo + 1; v <= hi; ++v) {
+    const int64_t w = v == n ? 0 : v;
+    for (int a = 0; a < 3; ++a) {
+      const double x = V[3 * w + a];
+      P.lo[a] = fmin(P.lo[a], x);
+      P.hi[a] = fmax(P.hi[a], x);
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    P.mid[a] = 0.5 * (P.hi[a] + P.lo[a]);
+    P.t[a] = 0.0;
+  }
+  for (int a = 0; a < 9; ++a) P.D[a] = 0.0;
+  for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int32_t sg = lo; sg < hi; ++sg) {
+    const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
+    double t[3], r[3];
+    for (int a = 0; a < 3; ++a) {
+      const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
+      t[a] = p1 - p0;
+      r[a] = (0.5 * p0 + 0.5 * p1) - P.mid[a];
+    }
+    for (int a = 0; a < 3; ++a) P.t[a] += t[a];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) P.D[3 * a + b] += t[a] * r[b];
+    for (int kk = 0; kk < 3; ++kk)
+      for (int q = 0; q < 6; ++q) {
+        const int i = ii[q], j = jj[q];
+        P.Q[6 * kk + q] += ((1.0 / 12.0) * t[kk]) * (t[i] * t[j]) + t[kk] * (r[i] * r[j]);
+      }
+  }
+  P.seg_lo = lo;
+  P.seg_cnt = hi - lo;
+  if (need) put16(A.bn + g, P);
+  const int32_t cl = A.children[2 * (base + node)], cr = A.children[2 * (base + node) + 1];
+  finish_record(P, A.hdr[base + node], A.mom[base + node], false, 0, cl, cr);
 }
 
 __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count) {
@@ -1211,7 +1288,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { travers
 #endif
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true>(A); }
 // Four CTAs per SM, as the plain kernel gets with its natural register count.
-__global__ void __launch_bounds__(32 * kWarps, 4) bh_traverse_learned(TravArgs A) { traverse<true, false>(A); }
+__global__ void __launch_bounds__(32 * kWarps, 3) bh_traverse_learned(TravArgs A) { traverse<true, false>(A); }
 
 // ------------------------------------------------------------------ split evaluation
 // Rounds with the evaluation taken out of the traversal: bh_classify walks
@@ -2102,9 +2179,11 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     int32_t *d_hcnt = ctx.d_bh[18].as<int32_t>(3 * 64);
     int32_t *d_hoff = d_hcnt + 64, *d_hcur = d_hcnt + 128;
     int32_t *d_bucket = ctx.d_bh[19].as<int32_t>(std::max<int64_t>(tot_int, 1));
+    int2 *d_range = ctx.d_bh[22].as<int2>(std::max<int64_t>(tot_int, 1));
     FLN_CUDA(cudaMemsetAsync(d_hcnt, 0, 3 * 64 * sizeof(int32_t), st));
     if (tot_int > 0)
-      curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int, d_height, d_hcnt);
+      curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int, d_height, d_hcnt,
+                                                                        d_range);
     identity_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
     build_moments<<<(int)((tot_leaf + 127) / 128), 128, 0, st>>>(T, d_segall, tot_leaf, false);
     FLN_CUDA(cudaGetLastError());
@@ -2122,7 +2201,12 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       FLN_CUDA(cudaMemcpyAsync(d_hoff, hoff, sizeof hoff, cudaMemcpyHostToDevice, st));
       bucket_heights<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(d_height, tot_int, d_hoff, d_hcur, d_bucket);
       ++launches;
-      for (int h = 1; h < 64; ++h) {
+      const int64_t nsmall = (int64_t)hoff[kSmallHeight + 1] - hoff[1];  // heights 1..kSmallHeight
+      if (nsmall > 0) {
+        build_small<<<(int)((nsmall + 127) / 128), 128, 0, st>>>(T, d_segint, d_bucket + hoff[1], nsmall, d_range);
+        ++launches;
+      }
+      for (int h = kSmallHeight + 1; h < 64; ++h) {
         if (!hcnt[h]) continue;
         build_height<<<(hcnt[h] + 127) / 128, 128, 0, st>>>(T, d_segint, d_bucket + hoff[h], hcnt[h]);
         ++launches;
