@@ -436,7 +436,7 @@ def main():
     ap.add_argument("--loop-steps", type=int, default=50000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
-    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=95.1,
+    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=94.1,
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
     ap.add_argument("--cli-leg", type=int, default=1,
                     help="also time the verifycurves CLI end to end on the workload written as BCC")
