@@ -104,7 +104,8 @@ typedef struct fln_stats {
   int64_t fp64_recomputed;      /* pairs recomputed in FP64 */
   int64_t beta_retried;         /* Barnes–Hut pairs re-run with a larger beta */
   double bh_far_evals;          /* Barnes–Hut far-field node pairs evaluated */
-  double bh_leaf_evals;         /* Barnes–Hut leaf-leaf segment pairs evaluated */
+  double bh_leaf_evals;         /* Barnes–Hut segment pairs summed exactly (leaf pairs and the segment
+                                   pairs of small node pairs, see bh_bucket) */
   double near_fp64_terms;       /* mixed direct sum: segment pairs evaluated in FP64 */
   double ms_kernels;            /* device time of the linking-number kernels (CUDA events) */
   double ms_total;              /* wall time of the last call */
