@@ -928,6 +928,152 @@ double bh_eval(const SegTree &t1, const SegTree &t2, double epssq, double itolsq
   return out;
 }
 
+// ------------------------------------------------- curve-order Barnes–Hut
+// The product's default Barnes–Hut (no counterpart in the reference; its
+// pieces follow the reference): a curve-order tree per loop (node = a
+// contiguous segment range, split at lo + (hi - lo) / 2; the internal node
+// that splits at s has id s - 1, the leaf of segment p has id n - 1 + p), the
+// moment build and shift of compute_link.cpp:333-389, the far field and
+// Eq. 14 estimate of :411-524, the exact term of :576-606. Node pairs that are
+// neither far nor leaf pairs and have at most `bucket` segments a side are
+// summed exactly over their segment pairs; bucket 1 is the reference's rule.
+// The roles of the two trees stay fixed (the product's traversal); the split
+// rule is the reference's (larger squared radius, or the internal node of an
+// internal/leaf pair). Everything in FP64, one pass at the given beta.
+CurveTree make_curve_tree(const Curve &c) {
+  if (c.type != SegType::Polyline) throw std::runtime_error("curve-order trees take polylines.");
+  CurveTree t;
+  const int n = (int)c.q.size();
+  t.n = n;
+  if (n < 2) throw std::runtime_error("Barnes-Hut needs loops of at least two segments.");
+  t.lo.assign(2 * n - 1, 0);
+  t.cnt.assign(2 * n - 1, 0);
+  t.left.assign(2 * n - 1, -1);
+  t.right.assign(2 * n - 1, -1);
+  t.box.assign(2 * n - 1, Box());
+  t.mom.assign(2 * n - 1, Moment());
+  const std::vector<V3> mids = c.midpoints(), tans = c.tangents();
+  struct B {
+    CurveTree &t;
+    const Curve &c;
+    const std::vector<V3> &mids, &tans;
+    int go(int lo, int hi) {
+      const int n = t.n;
+      if (hi - lo == 1) {
+        const int id = n - 1 + lo;
+        t.lo[id] = lo;
+        t.cnt[id] = 1;
+        t.box[id] = c.seg_box(lo);
+        Moment &C = t.mom[id];
+        C.mid = mids[lo];
+        const V3 c1 = tans[lo];
+        C.tan = c1;
+        C.tannorm = norm(c1);
+        const double cc[3] = {c1.x, c1.y, c1.z};
+        for (int r = 0; r < 3; ++r)
+          for (int q = 0; q < 3; ++q) {
+            const double o = cc[r] * cc[q];
+            C.q0[3 * r + q] = ((1.0 / 12.0) * cc[0]) * o;
+            C.q1[3 * r + q] = ((1.0 / 12.0) * cc[1]) * o;
+            C.q2[3 * r + q] = ((1.0 / 12.0) * cc[2]) * o;
+          }
+        C.quadnorm = (1.0 / 36.0) * C.tannorm * C.tannorm * C.tannorm;
+        return id;
+      }
+      const int s = lo + (hi - lo) / 2, id = s - 1;
+      const int l = go(lo, s), r = go(s, hi);
+      t.lo[id] = lo;
+      t.cnt[id] = hi - lo;
+      t.left[id] = l;
+      t.right[id] = r;
+      t.box[id] = box_merged(t.box[l], t.box[r]);
+      const Box &bb = t.box[id];
+      const V3 mid = 0.5 * (bb.hi + bb.lo);
+      Moment &M = t.mom[id];
+      M.mid = mid;
+      for (int ch : {l, r}) {
+        const Moment &C = t.mom[ch];
+        const V3 cv = C.tan;
+        M.tan = M.tan + cv;
+        const V3 rc = C.mid - mid;
+        const double c3[3] = {cv.x, cv.y, cv.z}, r3[3] = {rc.x, rc.y, rc.z};
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) M.dip[3 * a + b] += C.dip[3 * a + b] + c3[a] * r3[b];
+        double *MQ[3] = {M.q0, M.q1, M.q2};
+        const double *CQ[3] = {C.q0, C.q1, C.q2};
+        for (int k = 0; k < 3; ++k)
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              MQ[k][3 * a + b] += ((CQ[k][3 * a + b] + r3[b] * C.dip[3 * k + a]) + r3[a] * C.dip[3 * k + b]) +
+                                  c3[k] * (r3[a] * r3[b]);
+      }
+      M.tannorm = norm(M.tan);
+      double sd = 0, sq = 0;
+      for (int e = 0; e < 9; ++e) sd += M.dip[e] * M.dip[e];
+      for (int e = 0; e < 9; ++e) sq += M.q0[e] * M.q0[e] + M.q1[e] * M.q1[e] + M.q2[e] * M.q2[e];
+      M.dipnorm = std::sqrt(sd) * kInvRt3;
+      M.quadnorm = (1.0 / 3.0) * std::sqrt(sq);
+      return id;
+    }
+  } b{t, c, mids, tans};
+  t.root = b.go(0, n);
+  return t;
+}
+
+namespace {
+struct CurveBH {
+  const CurveTree &t1, &t2;
+  double epssq, itolsq;
+  int bucket;
+  double err = 0;
+  uint64_t nfar = 0, nexact = 0;
+  double exact(int s1, int s2) {
+    ++nexact;
+    return leaf_term(t1.mom[t1.n - 1 + s1], t2.mom[t2.n - 1 + s2]);
+  }
+  double rec(int a, int b) {
+    const Box &b1 = t1.box[a], &b2 = t2.box[b];
+    const double r1sq = 0.25 * dot(b1.hi - b1.lo, b1.hi - b1.lo);
+    const double r2sq = 0.25 * dot(b2.hi - b2.lo, b2.hi - b2.lo);
+    const double r1 = std::sqrt(r1sq), r2 = std::sqrt(r2sq);
+    const Moment &m1 = t1.mom[a], &m2 = t2.mom[b];
+    const V3 dr = m2.mid - m1.mid;
+    const double dsq = dot(dr, dr) + epssq;
+    const bool leaf1 = t1.left[a] < 0, leaf2 = t2.left[b] < 0;
+    if (leaf1 && leaf2) return exact(t1.lo[a], t2.lo[b]);
+    if (dsq > (r1 + r2) * (r1 + r2) * itolsq + epssq) {
+      ++nfar;
+      double res = dot(dr, cross(m2.tan, m1.tan));
+      const double rdist2 = 1.0 / dsq;
+      const double mult = rdist2 / std::sqrt(dsq) * kInvFourPi;
+      double e;
+      res += far_ho(m1, m2, dr, rdist2, r1, r2, e);
+      err += e * mult;
+      return mult * res;
+    }
+    if (t1.cnt[a] <= bucket && t2.cnt[b] <= bucket) {
+      double s = 0;
+      for (int i = 0; i < t1.cnt[a]; ++i)
+        for (int j = 0; j < t2.cnt[b]; ++j) s += exact(t1.lo[a] + i, t2.lo[b] + j);
+      return s;
+    }
+    const bool split2 = (!leaf1 && !leaf2) ? (r2sq > r1sq) : !leaf2;
+    if (split2) return rec(a, t2.left[b]) + rec(a, t2.right[b]);
+    return rec(t1.left[a], b) + rec(t1.right[a], b);
+  }
+};
+}  // namespace
+
+double curve_bh_eval(const CurveTree &t1, const CurveTree &t2, double epssq, double itolsq, int bucket,
+                     double &err, uint64_t *far_count, uint64_t *exact_count) {
+  CurveBH cx{t1, t2, epssq, itolsq, std::max(bucket, 1)};
+  const double v = cx.rec(t1.root, t2.root);
+  err = cx.err;
+  if (far_count) *far_count = cx.nfar;
+  if (exact_count) *exact_count = cx.nexact;
+  return v;
+}
+
 // ---------------------------------------------------------------- certificate
 std::string Certificate::text() const {
   std::ostringstream s;

@@ -106,6 +106,20 @@ SegTree make_seg_tree(const Curve &c);
 double bh_eval(const SegTree &t1, const SegTree &t2, double epssq, double itolsq, double &err,
                bool parallel, uint64_t *far_count = nullptr, uint64_t *leaf_count = nullptr);
 
+// The product's curve-order tree (no counterpart in the reference): node =
+// contiguous segment range; internal id = split - 1, leaf id = n - 1 + segment.
+struct CurveTree {
+  int n = 0, root = 0;
+  std::vector<int> lo, cnt, left, right;  // left < 0: leaf
+  std::vector<Box> box;
+  std::vector<Moment> mom;
+};
+CurveTree make_curve_tree(const Curve &c);
+// One Barnes–Hut pass over the two curve-order trees at itolsq = beta^2;
+// node pairs of at most `bucket` segments a side are summed exactly.
+double curve_bh_eval(const CurveTree &t1, const CurveTree &t2, double epssq, double itolsq, int bucket,
+                     double &err, uint64_t *far_count = nullptr, uint64_t *exact_count = nullptr);
+
 struct PairResult {
   int i, j;
   double lk;

@@ -21,6 +21,7 @@ struct OrcModel {
   std::vector<Curve> poly;        // after discretize (or copy)
   std::vector<std::pair<int, int>> pairs;  // unique potential links of `poly`
   std::vector<SegTree> trees;
+  std::vector<CurveTree> ctrees;  // curve-order trees of `poly`, built on first use
   int rounds = 0;
   std::string cert_text;
 };
@@ -83,6 +84,7 @@ int orc_prepare(void *m, int disc) {
     }
     o->pairs = potential_links_unique(o->poly);
     o->trees.clear();
+    o->ctrees.clear();
   });
 }
 
@@ -128,6 +130,7 @@ int orc_set_poly(void *m, int ncurves, const int64_t *offsets, const double *xyz
     }
     o->pairs = potential_links_unique(o->poly);
     o->trees.clear();
+    o->ctrees.clear();
   });
 }
 
@@ -187,6 +190,43 @@ int orc_eval_pairs(void *m, int method, const int32_t *pi, const int32_t *pj, in
       }
     }
     if (!err.empty()) throw std::runtime_error(err);
+  });
+}
+
+// One pass of the product's curve-order Barnes–Hut (see curve_bh_eval) per
+// pair at beta; out_err is the Eq. 14 estimate times 0.05 (lnc.cpp:165).
+int orc_eval_curve_bh(void *m, const int32_t *pi, const int32_t *pj, int64_t n, double beta, int bucket,
+                      int nthreads, double *out_lk, double *out_err, uint64_t *out_far, uint64_t *out_exact) {
+  return guard([&] {
+    auto *o = static_cast<OrcModel *>(m);
+    const int nc = (int)o->poly.size();
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    if ((int)o->ctrees.size() != nc) o->ctrees.assign(nc, CurveTree());
+    std::vector<char> need(nc, 0);
+    for (int64_t p = 0; p < n; ++p) {
+      if (pi[p] < 0 || pi[p] >= nc || pj[p] < 0 || pj[p] >= nc) throw std::runtime_error("pair out of range");
+      need[pi[p]] = need[pj[p]] = 1;
+    }
+    std::string err;
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < nc; ++i) {
+      try {
+        if (need[i] && o->ctrees[i].mom.empty()) o->ctrees[i] = make_curve_tree(o->poly[i]);
+      } catch (const std::exception &ex) {
+#pragma omp critical
+        err = ex.what();
+      }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t p = 0; p < n; ++p) {
+      double e = 0;
+      uint64_t nf = 0, nx = 0;
+      out_lk[p] = curve_bh_eval(o->ctrees[pi[p]], o->ctrees[pj[p]], 1e-24, beta * beta, bucket, e, &nf, &nx);
+      if (out_err) out_err[p] = 0.05 * e;
+      if (out_far) out_far[p] = nf;
+      if (out_exact) out_exact[p] = nx;
+    }
   });
 }
 

@@ -248,6 +248,25 @@ def test_buckets_keep_integers(engine, name, golden_dir):
         assert s["bh_leaf_evals"] > s1["bh_leaf_evals"]
 
 
+@pytest.mark.parametrize("name", ["knittubebroken", "glove"])
+@pytest.mark.parametrize("bucket", [1, 8])
+def test_curve_order_barneshut_matches_oracle(engine, name, bucket, golden_dir):
+    # The default tree and traversal against the oracle's FP64 restatement of
+    # them (one pass at beta 2, no retry, no FP64 recompute): the same node
+    # pairs, so the sums agree up to the FP32 far field and exact terms, and
+    # the work counts agree up to node pairs on the opening boundary.
+    _, off, xyz, pairs = _prepared(name, golden_dir)
+    o = pyoracle.Oracle().set_polylines(off, xyz)
+    lk_o, err_o, far_o, ex_o = o.eval_curve_bh(pairs, beta=2.0, bucket=bucket)
+    lk, err, _ = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_bucket=bucket, target_error=1e30,
+                                        bh_escalations=0, fp64_margin=0.0, bh_err_limit=1e30)
+    s = engine.stats()
+    np.testing.assert_allclose(lk, lk_o, rtol=0, atol=2e-5)
+    np.testing.assert_allclose(err, err_o, rtol=1e-3, atol=1e-9)
+    assert abs(s["bh_far_evals"] - float(far_o.sum())) <= 1e-5 * float(far_o.sum()) + 2
+    assert abs(s["bh_leaf_evals"] - float(ex_o.sum())) <= 1e-5 * float(ex_o.sum()) + 64
+
+
 def test_buckets_ignored_on_reference_tree(engine, golden_dir):
     # The kd-median tree has no contiguous segment ranges: bh_bucket has no
     # effect there (leaf pairs only, the reference's traversal).

@@ -47,3 +47,24 @@ def test_committed_pair_sums_reproduce(name, golden_dir):
     method = pyoracle.DIRECT_ONE_ARCTAN if len(off) - 1 < 6 else pyoracle.DIRECT_FAST
     lk, _, _, _ = o.eval_pairs(method, pairs)
     np.testing.assert_allclose(lk, ref["lk_direct"], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("name", ["knittubebroken", "glove"])
+def test_oracle_curve_order_barneshut(name, golden_dir):
+    # The product's default Barnes-Hut, restated in FP64 in the oracle
+    # (curve-order trees, small node pairs summed exactly): within the
+    # Barnes-Hut target error (0.1, lnc.cpp:25) of the FP64 direct sums the
+    # reference's own certificates were made from, the same integers, and
+    # buckets replace far-field terms by exact segment pairs.
+    o = pyoracle.Oracle().load_bcc(golden_bcc(name, golden_dir)).prepare(True)
+    pairs = o.pairs()
+    ref = np.load(os.path.join(GOLDEN, "pairs", name + ".npz"))
+    runs = {b: o.eval_curve_bh(pairs, beta=2.0, bucket=b) for b in (1, 8)}
+    for b, (lk, err, nfar, nex) in runs.items():
+        assert np.array_equal(np.rint(lk), np.rint(ref["lk_direct"]))
+        assert np.abs(lk - ref["lk_direct"]).max() < 0.1
+        assert np.all(err >= 0)
+    assert runs[8][2].sum() < runs[1][2].sum()
+    assert runs[8][3].sum() > runs[1][3].sum()
+    # Bucket 8 sums more of each pair exactly: on average closer to the direct sum.
+    assert np.abs(runs[8][0] - ref["lk_direct"]).mean() <= np.abs(runs[1][0] - ref["lk_direct"]).mean()
