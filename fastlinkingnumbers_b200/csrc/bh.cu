@@ -2528,9 +2528,12 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   ctx.stats.bh_far_evals = far_leaf[0];
   ctx.stats.bh_leaf_evals = far_leaf[1];
   ctx.stats.bh_exact_entries = prm.bh_schedule == 0 ? far_leaf[5] : far_leaf[1];
-  if (status != 0)
+  if (status & 1)
     throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
                                             std::to_string(maxdepth) + ").");
+  if (status != 0)
+    throw Error(FLN_ERR_INTERNAL, "Barnes-Hut work list exceeded its capacity (status " + std::to_string(status) +
+                                      ").");
   return launches;
 }
 
