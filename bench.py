@@ -203,7 +203,7 @@ def run_ours(args, rank, world, local_rank):
     poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed + rank, args.loops, args.loop_steps, engine=eng)
     raw_curves = cfg.pop("_raw")
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
-                           bh_tree=args.bh_tree, bh_schedule=args.bh_schedule)
+                           bh_tree=args.bh_tree, bh_schedule=args.bh_schedule, bh_bucket=args.bh_bucket)
     tune = None
     if args.bh_budget:
         prm.bh_budget = args.bh_budget
@@ -318,7 +318,9 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(cfg, parallelism=f"replicas x{world}"),
         "impl_details": {"method": args.method, "precision": args.precision,
                          "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median",
-                         "schedule": ["rounds, fused evaluation", "persistent queue", "rounds, split evaluation"][args.bh_schedule]},
+                         "schedule": ["rounds, fused evaluation", "persistent queue", "rounds, split evaluation"][args.bh_schedule],
+                         "exact_bucket_segments": 1 if (args.bh_tree == 1 or args.bh_schedule != 0)
+                         else (args.bh_bucket or 8)},
         "certificate_ms": ms,
         "autotune": tune,
         "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
@@ -440,6 +442,8 @@ def main():
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
     ap.add_argument("--cli-leg", type=int, default=1,
                     help="also time the verifycurves CLI end to end on the workload written as BCC")
+    ap.add_argument("--bh-bucket", type=int, default=0,
+                    help="node pairs of at most this many segments a side are summed exactly; 0 = 8, 1 = leaf pairs only")
     ap.add_argument("--bh-budget", type=int, default=0,
                     help="fixed Barnes-Hut round budget (skips the autotuner); 0 = tuned")
     ap.add_argument("--autotune", type=int, default=1,
