@@ -68,3 +68,25 @@ def test_oracle_curve_order_barneshut(name, golden_dir):
     assert runs[8][3].sum() > runs[1][3].sum()
     # Bucket 8 sums more of each pair exactly: on average closer to the direct sum.
     assert np.abs(runs[8][0] - ref["lk_direct"]).mean() <= np.abs(runs[1][0] - ref["lk_direct"]).mean()
+
+
+@pytest.mark.parametrize("workload", ["ring_chain", "knots", "polymer"])
+def test_oracle_curve_order_barneshut_on_synthetic_loops(workload):
+    # The restated default Barnes-Hut on seeded synthetic loops (the ring
+    # chain of the benchmark suite, torus knots, interleaved walks): the
+    # integers of the oracle's FP64 direct sum for bucket 1 and 8.
+    from fastlinkingnumbers_b200 import workloads as W
+    if workload == "ring_chain":
+        off, xyz = W.ring_chain(seed=5)
+    elif workload == "knots":
+        off, xyz = W.mixed_batch(seed=5, n_loops=24, hi=2000, cube=30.0)
+    else:
+        off, xyz = W.polymer(seed=5, n_loops=6, n_steps=3000, cube=40.0)
+    o = pyoracle.Oracle().set_polylines(off, xyz)
+    pairs = o.pairs()
+    assert len(pairs) > 0
+    lk_d, _, _, _ = o.eval_pairs(pyoracle.DIRECT_FAST, pairs)
+    for b in (1, 8):
+        lk, err, nfar, nex = o.eval_curve_bh(pairs, beta=2.0, bucket=b)
+        assert np.array_equal(np.rint(lk), np.rint(lk_d))
+        assert np.abs(lk - lk_d).max() < 0.1
