@@ -2,7 +2,11 @@
 // certificates. Compiled with -ffp-contract=off (see geometry.hpp).
 #include "host.hpp"
 
+#include <fcntl.h>
 #include <omp.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -42,18 +46,40 @@ struct BccHeader {
 static_assert(sizeof(BccHeader) == 64, "BCC header size");
 }  // namespace
 
+// BCC reader (model.cpp:280-364): the file is mapped, one serial pass finds
+// where each curve's points start (the counts chain the records), and the
+// float32 points are widened to double in parallel. The same checks, in the
+// same order, as a record-by-record read.
 void load_bcc(const std::string &path, Model &m) {
-  FILE *f = std::fopen(path.c_str(), "rb");
-  if (!f) throw Error(FLN_ERR_IO, "Unable to open BCC file: " + path);
-  std::fseek(f, 0, SEEK_END);
-  const long long fsize = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
+  const int fd = ::open(path.c_str(), O_RDONLY);
+  if (fd < 0) throw Error(FLN_ERR_IO, "Unable to open BCC file: " + path);
+  struct stat st;
+  if (::fstat(fd, &st) != 0) {
+    ::close(fd);
+    throw Error(FLN_ERR_IO, "Unable to open BCC file: " + path);
+  }
+  const uint64_t fsize = (uint64_t)st.st_size;
+  const unsigned char *base = nullptr;
+  if (fsize > 0) {
+    void *mp = ::mmap(nullptr, fsize, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (mp == MAP_FAILED) {
+      ::close(fd);
+      throw Error(FLN_ERR_IO, "Unable to map BCC file: " + path);
+    }
+    base = static_cast<const unsigned char *>(mp);
+  }
+  ::close(fd);
+  struct Unmap {
+    const unsigned char *p;
+    uint64_t n;
+    ~Unmap() {
+      if (p) ::munmap(const_cast<unsigned char *>(p), n);
+    }
+  } unmap{base, fsize};
+  auto fail = [&](fln_status s, const std::string &msg) { throw Error(s, msg + ": " + path); };
   BccHeader h;
-  auto fail = [&](fln_status s, const std::string &msg) {
-    std::fclose(f);
-    throw Error(s, msg + ": " + path);
-  };
-  if (std::fread(&h, sizeof h, 1, f) != 1) fail(FLN_ERR_IO, "Incomplete BCC header");
+  if (fsize < sizeof h) fail(FLN_ERR_IO, "Incomplete BCC header");
+  std::memcpy(&h, base, sizeof h);
   if (h.sign[0] != 'B' || h.sign[1] != 'C' || h.sign[2] != 'C') fail(FLN_ERR_FORMAT, "Invalid BCC header");
   if (h.bytes != 0x44) fail(FLN_ERR_FORMAT, "Invalid BCC bytecount (only 32-bit ints and floats)");
   if (h.dims != 3) fail(FLN_ERR_FORMAT, "Invalid BCC dimensions (only 3D)");
@@ -65,23 +91,36 @@ void load_bcc(const std::string &path, Model &m) {
   else fail(FLN_ERR_FORMAT, "Invalid BCC curve type (only C0, BS, BZ, PL)");
   // Every curve needs at least its 4-byte count: reject impossible counts
   // before allocating.
-  if (h.ncurves > (uint64_t)std::max(0LL, fsize - 64) / 4) fail(FLN_ERR_FORMAT, "BCC curve count exceeds file size");
+  if (h.ncurves > (fsize - 64) / 4) fail(FLN_ERR_FORMAT, "BCC curve count exceeds file size");
+  std::vector<uint64_t> at(h.ncurves);  // byte offset of each curve's points
+  std::vector<int64_t> npts(h.ncurves);
   std::vector<CurveData> curves(h.ncurves);
-  std::vector<float> buf;
+  uint64_t p = sizeof h;
   for (uint64_t i = 0; i < h.ncurves; ++i) {
+    if (p + 4 > fsize) fail(FLN_ERR_IO, "Cannot read curve control point count");
     int32_t cnt;
-    if (std::fread(&cnt, 4, 1, f) != 1) fail(FLN_ERR_IO, "Cannot read curve control point count");
-    CurveData &c = curves[i];
-    c.kind = kind;
-    c.closed = cnt < 0;
+    std::memcpy(&cnt, base + p, 4);
     const int64_t n = cnt < 0 ? -(int64_t)cnt : cnt;
-    if (n * 12 > fsize) fail(FLN_ERR_FORMAT, "BCC point count exceeds file size");
-    buf.resize(3 * n);
-    if (n && std::fread(buf.data(), 4, 3 * n, f) != (size_t)(3 * n)) fail(FLN_ERR_IO, "Invalid number of control points read");
-    c.q.resize(n);
-    for (int64_t k = 0; k < n; ++k) c.q[k] = {(double)buf[3 * k], (double)buf[3 * k + 1], (double)buf[3 * k + 2]};
+    if ((uint64_t)n * 12 > fsize) fail(FLN_ERR_FORMAT, "BCC point count exceeds file size");
+    if (p + 4 + (uint64_t)n * 12 > fsize) fail(FLN_ERR_IO, "Invalid number of control points read");
+    curves[i].kind = kind;
+    curves[i].closed = cnt < 0;
+    at[i] = p + 4;
+    npts[i] = n;
+    p += 4 + (uint64_t)n * 12;
   }
-  std::fclose(f);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < (int64_t)h.ncurves; ++i) {
+    CurveData &c = curves[i];
+    const int64_t n = npts[i];
+    c.q.resize(n);
+    const unsigned char *src = base + at[i];
+    for (int64_t k = 0; k < n; ++k) {
+      float v[3];
+      std::memcpy(v, src + 12 * k, 12);
+      c.q[k] = {(double)v[0], (double)v[1], (double)v[2]};
+    }
+  }
   m.curves.swap(curves);
   m.prepared = false;
 }
