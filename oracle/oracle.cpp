@@ -1027,9 +1027,13 @@ struct CurveBH {
   int bucket;
   double err = 0;
   uint64_t nfar = 0, nexact = 0;
+  double exsum = 0;                                // the exact terms alone
+  std::vector<std::pair<int, int>> *far_pairs = nullptr;  // records the far node pairs if set
   double exact(int s1, int s2) {
     ++nexact;
-    return leaf_term(t1.mom[t1.n - 1 + s1], t2.mom[t2.n - 1 + s2]);
+    const double v = leaf_term(t1.mom[t1.n - 1 + s1], t2.mom[t2.n - 1 + s2]);
+    exsum += v;
+    return v;
   }
   double rec(int a, int b) {
     const Box &b1 = t1.box[a], &b2 = t2.box[b];
@@ -1043,6 +1047,7 @@ struct CurveBH {
     if (leaf1 && leaf2) return exact(t1.lo[a], t2.lo[b]);
     if (dsq > (r1 + r2) * (r1 + r2) * itolsq + epssq) {
       ++nfar;
+      if (far_pairs) far_pairs->push_back({a, b});
       double res = dot(dr, cross(m2.tan, m1.tan));
       const double rdist2 = 1.0 / dsq;
       const double mult = rdist2 / std::sqrt(dsq) * kInvFourPi;
@@ -1063,6 +1068,29 @@ struct CurveBH {
   }
 };
 }  // namespace
+
+// The same traversal at beta1 >= beta0, continued from a beta0 pass: a node
+// pair opened at beta0 is opened at beta1 (far at beta1 implies far at
+// beta0), and an exact pair stays exact (the bucket test does not depend on
+// beta). So the beta1 sum is the beta0 pass's exact terms plus the beta1
+// traversal of the beta0 pass's far pairs, node pair for node pair; err and
+// far_count are the continuation's, exact_count counts both passes.
+double curve_bh_eval_continued(const CurveTree &t1, const CurveTree &t2, double epssq, double itolsq0,
+                               double itolsq1, int bucket, double &err, uint64_t *far_count,
+                               uint64_t *exact_count) {
+  if (itolsq1 < itolsq0) throw std::runtime_error("the continued pass needs beta1 >= beta0");
+  std::vector<std::pair<int, int>> frontier;
+  CurveBH p0{t1, t2, epssq, itolsq0, std::max(bucket, 1)};
+  p0.far_pairs = &frontier;
+  p0.rec(t1.root, t2.root);
+  CurveBH p1{t1, t2, epssq, itolsq1, std::max(bucket, 1)};
+  double v = p0.exsum;
+  for (const auto &fp : frontier) v += p1.rec(fp.first, fp.second);
+  err = p1.err;
+  if (far_count) *far_count = p1.nfar;
+  if (exact_count) *exact_count = p0.nexact + p1.nexact;
+  return v;
+}
 
 double curve_bh_eval(const CurveTree &t1, const CurveTree &t2, double epssq, double itolsq, int bucket,
                      double &err, uint64_t *far_count, uint64_t *exact_count) {

@@ -119,6 +119,11 @@ CurveTree make_curve_tree(const Curve &c);
 // node pairs of at most `bucket` segments a side are summed exactly.
 double curve_bh_eval(const CurveTree &t1, const CurveTree &t2, double epssq, double itolsq, int bucket,
                      double &err, uint64_t *far_count = nullptr, uint64_t *exact_count = nullptr);
+// The same pass at itolsq1, continued from an itolsq0 pass's far node pairs
+// and reusing its exact terms (the node pairs are the same).
+double curve_bh_eval_continued(const CurveTree &t1, const CurveTree &t2, double epssq, double itolsq0,
+                               double itolsq1, int bucket, double &err, uint64_t *far_count = nullptr,
+                               uint64_t *exact_count = nullptr);
 
 struct PairResult {
   int i, j;

@@ -193,10 +193,22 @@ int orc_eval_pairs(void *m, int method, const int32_t *pi, const int32_t *pj, in
   });
 }
 
+int orc_eval_curve_bh2(void *m, const int32_t *pi, const int32_t *pj, int64_t n, double beta0, double beta,
+                       int bucket, int nthreads, double *out_lk, double *out_err, uint64_t *out_far,
+                       uint64_t *out_exact);
+
 // One pass of the product's curve-order Barnes–Hut (see curve_bh_eval) per
 // pair at beta; out_err is the Eq. 14 estimate times 0.05 (lnc.cpp:165).
 int orc_eval_curve_bh(void *m, const int32_t *pi, const int32_t *pj, int64_t n, double beta, int bucket,
                       int nthreads, double *out_lk, double *out_err, uint64_t *out_far, uint64_t *out_exact) {
+  return orc_eval_curve_bh2(m, pi, pj, n, beta, beta, bucket, nthreads, out_lk, out_err, out_far, out_exact);
+}
+
+// As orc_eval_curve_bh at beta1, continued from a pass at beta0 < beta1
+// (curve_bh_eval_continued); beta0 == beta1 is one plain pass.
+int orc_eval_curve_bh2(void *m, const int32_t *pi, const int32_t *pj, int64_t n, double beta0, double beta,
+                       int bucket, int nthreads, double *out_lk, double *out_err, uint64_t *out_far,
+                       uint64_t *out_exact) {
   return guard([&] {
     auto *o = static_cast<OrcModel *>(m);
     const int nc = (int)o->poly.size();
@@ -222,7 +234,10 @@ int orc_eval_curve_bh(void *m, const int32_t *pi, const int32_t *pj, int64_t n, 
     for (int64_t p = 0; p < n; ++p) {
       double e = 0;
       uint64_t nf = 0, nx = 0;
-      out_lk[p] = curve_bh_eval(o->ctrees[pi[p]], o->ctrees[pj[p]], 1e-24, beta * beta, bucket, e, &nf, &nx);
+      out_lk[p] = beta0 < beta ? curve_bh_eval_continued(o->ctrees[pi[p]], o->ctrees[pj[p]], 1e-24, beta0 * beta0,
+                                                         beta * beta, bucket, e, &nf, &nx)
+                               : curve_bh_eval(o->ctrees[pi[p]], o->ctrees[pj[p]], 1e-24, beta * beta, bucket, e,
+                                               &nf, &nx);
       if (out_err) out_err[p] = 0.05 * e;
       if (out_far) out_far[p] = nf;
       if (out_exact) out_exact[p] = nx;

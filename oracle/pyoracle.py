@@ -57,6 +57,8 @@ def lib():
                                      C.c_int, C.c_int, f64p, f64p, u64p, u64p]
         L.orc_eval_curve_bh.argtypes = [vp, i32p, i32p, C.c_int64, C.c_double, C.c_int, C.c_int,
                                          f64p, f64p, u64p, u64p]
+        L.orc_eval_curve_bh2.argtypes = [vp, i32p, i32p, C.c_int64, C.c_double, C.c_double, C.c_int, C.c_int,
+                                          f64p, f64p, u64p, u64p]
         L.orc_certificate.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, f64p, f64p]
         L.orc_certificate_text.argtypes = [vp, C.c_char_p]
         L.orc_certificate.restype = C.c_int64
@@ -150,9 +152,11 @@ class Oracle:
                 _p(nfar, C.c_uint64), _p(nleaf, C.c_uint64)))
         return lk, err, nfar, nleaf
 
-    def eval_curve_bh(self, pairs, beta=2.0, bucket=8, nthreads=0):
+    def eval_curve_bh(self, pairs, beta=2.0, bucket=8, nthreads=0, continue_from=None):
         """One pass of the product's curve-order Barnes-Hut (FP64) per pair:
-        (lk, err * 0.05, far node pairs, exact segment pairs)."""
+        (lk, err * 0.05, far node pairs, exact segment pairs). With
+        continue_from = beta0 < beta, the pass at beta is continued from a
+        pass at beta0 (its far node pairs, its exact terms reused)."""
         pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
         pi = np.ascontiguousarray(pairs[:, 0])
         pj = np.ascontiguousarray(pairs[:, 1])
@@ -162,8 +166,9 @@ class Oracle:
         nfar = np.zeros(n, dtype=np.uint64)
         nex = np.zeros(n, dtype=np.uint64)
         if n:
-            self._check(self._L.orc_eval_curve_bh(
-                self._h, _p(pi, C.c_int32), _p(pj, C.c_int32), n, beta, int(bucket), nthreads,
+            b0 = beta if continue_from is None else continue_from
+            self._check(self._L.orc_eval_curve_bh2(
+                self._h, _p(pi, C.c_int32), _p(pj, C.c_int32), n, b0, beta, int(bucket), nthreads,
                 _p(lk, C.c_double), _p(err, C.c_double), _p(nfar, C.c_uint64), _p(nex, C.c_uint64)))
         return lk, err, nfar, nex
 

@@ -90,3 +90,22 @@ def test_oracle_curve_order_barneshut_on_synthetic_loops(workload):
         lk, err, nfar, nex = o.eval_curve_bh(pairs, beta=2.0, bucket=b)
         assert np.array_equal(np.rint(lk), np.rint(lk_d))
         assert np.abs(lk - lk_d).max() < 0.1
+
+
+@pytest.mark.parametrize("bucket", [1, 8])
+def test_beta_retry_continues_from_the_first_pass(bucket, golden_dir):
+    # The retry pass at beta* visits the same node pairs whether it starts
+    # from the roots or from the beta0 pass's far node pairs with that pass's
+    # exact terms reused: same sums (to FP64 summation order), same error
+    # estimate, same far-field and exact counts.
+    from fastlinkingnumbers_b200 import workloads as W
+    off, xyz = W.polymer(seed=9, n_loops=6, n_steps=4000, cube=45.0)
+    o = pyoracle.Oracle().set_polylines(off, xyz)
+    pairs = o.pairs()
+    assert len(pairs) > 5
+    for beta in (2.3, 3.0, 10.0):
+        lk, err, nf, nx = o.eval_curve_bh(pairs, beta=beta, bucket=bucket)
+        lkc, errc, nfc, nxc = o.eval_curve_bh(pairs, beta=beta, bucket=bucket, continue_from=2.0)
+        np.testing.assert_allclose(lkc, lk, rtol=0, atol=1e-10)
+        np.testing.assert_allclose(errc, err, rtol=1e-10, atol=1e-15)
+        assert np.array_equal(nfc, nf) and np.array_equal(nxc, nx)
