@@ -53,33 +53,26 @@ def _peaks():
         return PEAKS_FALLBACK, "fallback"
 
 
-def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000, engine=None):
-    from fastlinkingnumbers_b200 import Model, workloads as W
-    if name == "polymer":
+def _workload_curves(name: str, seed: int, loops: int, steps: int):
+    """The seeded curves of a workload (numpy only: loads no native library)."""
+    from fastlinkingnumbers_b200 import workloads as W
+    if name == "polymer" and (loops, steps) != (200, 50000):
         off, xyz = W.polymer(seed=seed, n_loops=loops, n_steps=steps)
-        cfg = {"workload": f"polymer loops: {loops} x {steps}-step closed Gaussian walks "
-                           f"({loops * steps / 1e6:g}M segments), cube 400",
-               "loops": loops, "steps_per_loop": steps}
-    elif name == "held_out_20M":
-        # Held-out evaluation set of the learned criterion: 1,000 walks of
-        # 20,000 steps at the polymer workload's density (cube 400 x 2^(1/3)).
-        off, xyz = W.polymer(seed=seed, n_loops=1000, n_steps=20000, cube=504.0)
-        cfg = {"workload": "held-out polymer: 1000 x 20000-step closed Gaussian walks (20M segments), "
-                           "cube 504", "loops": 1000, "steps_per_loop": 20000}
-    elif name == "mixed_batch":
-        off, xyz = W.mixed_batch(seed=seed)
-        cfg = {"workload": "mixed batch: 5000 loops, half (p,q) torus knots, half closed walks, sizes "
-                           "log-uniform in [16, 2^18] (134M segments), cube 600", "loops": 5000}
-    elif name == "chain_mail":
-        off, xyz = W.chain_mail(seed=seed)
-        cfg = {"workload": "chain-mail sheet: 100 x 100 rings, 48-gons (480k segments)", "loops": 10000}
-    elif name == "ring_chain":
-        off, xyz = W.ring_chain(seed=seed)
-        cfg = {"workload": "ring chain: 64 rings x 32 segments", "loops": 64}
+        desc = (f"polymer loops: {loops} x {steps}-step closed Gaussian walks "
+                f"({loops * steps / 1e6:g}M segments), cube 400")
     else:
-        raise SystemExit(f"unknown workload {name}")
+        off, xyz, desc = W.named(name, seed)
+    cfg = {"workload": desc, "loops": int(len(off) - 1)}
+    if name == "polymer":
+        cfg["steps_per_loop"] = steps
     cfg.update({"method": "barneshut (quadrupole, beta 2, beta_limit 10)", "seed": seed,
                 "l2": "inputs and per-step trees larger than L2 (no flush needed)"})
+    return off, xyz, cfg
+
+
+def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000, engine=None):
+    from fastlinkingnumbers_b200 import Model
+    off, xyz, cfg = _workload_curves(name, seed, loops, steps)
     m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
     t0 = time.perf_counter()
     poff, pxyz, pairs, rounds = m.Prepare(True, engine=engine)
@@ -135,12 +128,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_sample_run(poff, pxyz, pairs, target_s: float, seed: int, nthreads: int):
+def cpu_sample_run(poff, pxyz, pairs, target_s: float, seed: int, nthreads: int, oracle=None):
     """Times the oracle (the reference's CPU algorithm: loop-pair parallel,
-    serial depth-first Barnes–Hut with the beta retry) on a seeded sample of
-    pairs sized for about target_s seconds; returns (Gsegpair/s, info)."""
+    serial depth-first Barnes–Hut with the beta retry; built -O3
+    -march=native like the reference) on a seeded sample of pairs sized for
+    about target_s seconds; returns (Gsegpair/s, info)."""
     from oracle import pyoracle
-    o = pyoracle.Oracle().set_polylines(poff, pxyz)
+    o = oracle if oracle is not None else pyoracle.Oracle(native=True).set_polylines(poff, pxyz)
     rng = np.random.default_rng(seed)
     order = rng.permutation(len(pairs))
     n = np.diff(poff).astype(np.float64)
@@ -160,29 +154,49 @@ def cpu_sample_run(poff, pxyz, pairs, target_s: float, seed: int, nthreads: int)
 
 
 def run_reference(args, rank):
+    """The reference's CPU path, restated by the oracle, end to end on the
+    host: the oracle generates nothing itself, so the seeded curves come from
+    the workload generator (numpy); the oracle then runs the reference's
+    potential-link search and Discretize, and each step times its Barnes-Hut
+    over a seeded sample of the pairs. No product library is loaded."""
     if rank != 0:
         return
-    poff, pxyz, pairs, cfg = make_workload(args.workload, args.seed, args.loops, args.loop_steps)
-    cfg.pop("_raw", None)
     from oracle import pyoracle
-    threads = pyoracle.max_threads()
+    off, xyz, cfg = _workload_curves(args.workload, args.seed, args.loops, args.loop_steps)
+    o = pyoracle.Oracle(native=True).set_curves(pyoracle.SEG_POLYLINE, -np.diff(off).astype(np.int32), xyz)
+    del xyz
+    t0 = time.perf_counter()
+    o.prepare(True)
+    cfg["prepare_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+    cfg["prepare_on"] = "host (oracle)"
+    cfg["discretize_rounds"] = int(o.rounds)
+    poff, pxyz = o.polylines()
+    pairs = o.pairs()
+    cfg["segments_after_discretize"] = int(poff[-1])
+    cfg["pairs"] = int(len(pairs))
+    threads = pyoracle.max_threads(native=True)
+    # Each step is a bounded sample, sized so that the whole run stays within
+    # about four minutes.
+    per_step = min(args.cpu_seconds, max(3.0, 240.0 / max(1, args.steps + args.warmup)))
     vals = []
     for s in range(args.warmup + args.steps):
-        v, info = cpu_sample_run(poff, pxyz, pairs, args.cpu_seconds, args.seed + 17, threads)
+        v, info = cpu_sample_run(poff, pxyz, pairs, per_step, args.seed + 17, threads, oracle=o)
         if s >= args.warmup:
             vals.append((v, info))
     v = float(np.mean([x[0] for x in vals]))
     info = vals[-1][1]
     sample = (f"{info['pairs']} seeded random pairs of {len(pairs)} ({info['segment_pairs']:.3g} "
-              f"segment pairs), Barnes-Hut beta 2 with retry, oracle port of the reference")
+              f"segment pairs, {info['seconds']} s) per step, Barnes-Hut beta 2 with retry, oracle port of "
+              f"the reference built -O3 -march=native")
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * info["seconds"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "ms_per_step": 1e3 * float(np.mean([x[1]["seconds"] for x in vals])), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": dict(cfg, parallelism=f"replicas x{args.gpus}"),
         "impl_details": {"method": "barneshut", "precision": "f64",
-                         "tree": "reference kd-median", "traversal": "serial depth-first per pair"},
+                         "tree": "reference kd-median", "traversal": "serial depth-first per pair",
+                         "prepare": "oracle potential-link search + Discretize (host)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -409,12 +423,13 @@ def run_ours(args, rank, world, local_rank):
                              "same_entry_count_as_bench": entries == int(np.sum(np.round(lk) != 0))}
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         from oracle import pyoracle
-        thr = pyoracle.max_threads()
+        thr = pyoracle.max_threads(native=True)
         v, info = cpu_sample_run(poff, pxyz, pairs, args.cpu_seconds, args.seed + 17, thr)
         result["cpu_baseline"] = {
             "value": v, "unit": UNIT, "cores": thr, "kind": "port",
             "sample": f"{info['pairs']} seeded random pairs ({info['segment_pairs']:.3g} segment "
-                      f"pairs) in {info['seconds']} s; oracle port of the reference's BH"}
+                      f"pairs) in {info['seconds']} s; oracle port of the reference's BH, built -O3 "
+                      f"-march=native"}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -377,7 +377,7 @@ void fln_default_params(fln_params *p) {
   p->error_est_scale = 0.05;
   p->precision = FLN_PREC_MIXED;
   p->fp64_margin = 0.25;
-  p->near_factor = 4.0;
+  p->near_factor = kDefaultNearFactor;
   p->bh_tree = 0;
   p->bh_escalations = 2;
   p->bh_err_limit = 0.25;

@@ -473,7 +473,13 @@ int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
 // process exits. Limits: at most kNoAllocMaxPairs loop pairs per call and
 // kNoAllocMaxItems work items (one item = 128 segments of the longer loop of
 // a pair, summed over the pairs); larger calls are rejected with
-// FLN_ERR_INVALID_ARGUMENT before any kernel runs on them.
+// FLN_ERR_INVALID_ARGUMENT before any kernel runs on them. The mixed
+// precision uses the default near factor (kDefaultNearFactor), so results
+// equal the allocating entry point's with fln_default_params.
+//
+// Every call copies the plan's header (item count, status) back to the host
+// and waits for it: the call blocks until the work queued earlier on the
+// stream and the planning kernel have run.
 //
 // In host code the name g_noalloc_scratch only stands for the array: its
 // device address is obtained once per device with cudaGetSymbolAddress, on
@@ -651,7 +657,7 @@ extern "C" fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, co
   DirectArgs A{d_xyz, d_loop_offsets, reinterpret_cast<const int32_t *>(scratch + kNaLoops),
                reinterpret_cast<const int64_t *>(scratch + kNaStart), (int32_t)npairs, h.total_items,
                reinterpret_cast<double *>(scratch + kNaPartial), reinterpret_cast<unsigned long long *>(scratch),
-               1.0f};
+               (float)kDefaultNearFactor};
   if (precision == FLN_PREC_FP64) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel, kBlockSegs, 0);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));

@@ -125,6 +125,12 @@ struct Context {
   ~Context();
 };
 
+// Mixed direct sum: a segment pair whose closest endpoint distance is below
+// this multiple of the longer segment's length is evaluated in FP64 (the
+// default of fln_params.near_factor, and the factor of the allocation-free
+// entry point).
+constexpr double kDefaultNearFactor = 4.0;
+
 // Plans and runs the direct sum over `npairs` pairs of the loops in device
 // memory. d_xyz/d_off describe the loops; h_off is the host copy of the
 // offsets; h_pairs the host copy of the pairs. Writes lk (per caller pair) to

@@ -109,11 +109,13 @@ void load_bcc(const std::string &path, Model &m) {
     npts[i] = n;
     p += 4 + (uint64_t)n * 12;
   }
+  // Allocate here, serially: an allocation failure inside the parallel
+  // region could not leave it as an exception.
+  for (uint64_t i = 0; i < h.ncurves; ++i) curves[i].q.resize(npts[i]);
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t i = 0; i < (int64_t)h.ncurves; ++i) {
     CurveData &c = curves[i];
     const int64_t n = npts[i];
-    c.q.resize(n);
     const unsigned char *src = base + at[i];
     for (int64_t k = 0; k < n; ++k) {
       float v[3];

@@ -180,6 +180,71 @@ def write_bcc(path, loops_or_packed, seg_type="PL"):
             f.write(np.asarray(l, dtype=np.float32).tobytes())
 
 
+def named(name: str, seed: int = 3):
+    """The benchmark workloads by name: (loop_offsets, xyz, description).
+
+      ring_chain    64 rings x 32 segments
+      chain_mail    100 x 100 rings, 48-gons (480k segments)
+      polymer       200 x 50,000-step closed walks (10M segments), cube 400
+      held_out_20M  1,000 x 20,000-step closed walks (20M segments), cube 504:
+                    the polymer density, the learned criterion's held-out set
+      mixed_batch   5,000 torus knots and walks, 16 to 2^18 segments (134M
+                    segments), cube 600
+    """
+    if name == "polymer":
+        off, xyz = polymer(seed=seed, n_loops=200, n_steps=50_000, cube=400.0)
+        d = "polymer loops: 200 x 50000-step closed Gaussian walks (10M segments), cube 400"
+    elif name == "held_out_20M":
+        off, xyz = polymer(seed=seed, n_loops=1000, n_steps=20_000, cube=504.0)
+        d = "held-out polymer: 1000 x 20000-step closed Gaussian walks (20M segments), cube 504"
+    elif name == "mixed_batch":
+        off, xyz = mixed_batch(seed=seed)
+        d = ("mixed batch: 5000 loops, half (p,q) torus knots, half closed walks, sizes log-uniform in "
+             "[16, 2^18] (134M segments), cube 600")
+    elif name == "chain_mail":
+        off, xyz = chain_mail(seed=seed)
+        d = "chain-mail sheet: 100 x 100 rings, 48-gons (480k segments)"
+    elif name == "ring_chain":
+        off, xyz = ring_chain(seed=seed)
+        d = "ring chain: 64 rings x 32 segments"
+    else:
+        raise ValueError(f"unknown workload {name}")
+    return off, xyz, d
+
+
+def digest(*arrays) -> str:
+    """SHA-256 (hex, first 32 digits) of the arrays' bytes: pins a prepared
+    workload (polylines and pairs) between machines."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        a = np.ascontiguousarray(a)
+        h.update(str(a.dtype).encode() + str(a.shape).encode())
+        mv = memoryview(a).cast("B")
+        for k in range(0, len(mv), 1 << 28):
+            h.update(mv[k:k + (1 << 28)])
+    return h.hexdigest()[:32]
+
+
+def certificate_text(ncurves: int, pairs, lk) -> str:
+    """Certificate text from per-pair real sums, as ExportToFile writes it
+    (linking_number_certificate.cpp:185-213, :441-454): the curve count, then
+    `i,j,lk` for every pair whose std::round (half away from zero) is
+    nonzero, with i < j, sorted by (i, j)."""
+    pairs = np.asarray(pairs).reshape(-1, 2)
+    lk = np.asarray(lk, dtype=np.float64)
+    r = np.sign(lk) * np.floor(np.abs(lk) + 0.5)
+    if not np.all(np.isfinite(r)):
+        raise ValueError("non-finite linking number")
+    keep = np.abs(r) >= 0.25
+    i = np.minimum(pairs[keep, 0], pairs[keep, 1])
+    j = np.maximum(pairs[keep, 0], pairs[keep, 1])
+    v = r[keep].astype(np.int64)
+    o = np.lexsort((j, i))
+    lines = [str(int(ncurves))] + [f"{a},{b},{c}" for a, b, c in zip(i[o], j[o], v[o])]
+    return "\n".join(lines) + "\n"
+
+
 def pair_work(off, pairs):
     """Sum over pairs of n_i * n_j (direct-sum-equivalent segment pairs)."""
     n = np.diff(off).astype(np.float64)

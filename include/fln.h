@@ -175,9 +175,13 @@ fln_status fln_linking_numbers_device(fln_ctx *ctx, const double *d_xyz,
  * work items (one item = 128 segments of the longer loop of a pair, summed
  * over pairs); larger calls return FLN_ERR_INVALID_ARGUMENT. precision is
  * FLN_PREC_FP64 or FLN_PREC_MIXED; the results are the raw sums of that
- * precision (no margin recompute). Work is queued on `stream` (a
- * cudaStream_t, NULL = default stream) of the current device; the call
- * waits for a small planning step and returns with the sums still in flight
+ * precision (no margin recompute), the mixed one with the default
+ * near_factor, 4.0, so they equal those of fln_linking_numbers_device with
+ * the same precision and fp64_margin = 0. Work is queued on `stream` (a
+ * cudaStream_t, NULL = default stream) of the current device. Every call
+ * reads the plan's size and status back to the host, so it blocks the
+ * calling thread until the work queued earlier on `stream` and a small
+ * planning kernel have finished; it returns with the sums still in flight
  * on `stream`. The first call on a device looks up the array's device
  * address, so make it before any stream capture. Calls share the array:
  * calls whose work overlaps on the GPU race, so issue them one at a time. */

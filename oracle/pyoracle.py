@@ -17,7 +17,13 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
-_lib = None
+_libs = {}
+# The reference is built -O3 -march=native (its CMakeLists.txt:19). The timed
+# CPU baseline uses the same flags (plus -ffp-contract=off, as every oracle
+# build), compiled on the host that runs it into a folder keyed by that
+# host's CPU, so a library built for one CPU is never loaded on another. The
+# checker in the tests uses the portable x86-64-v3 build.
+_NATIVE_FLAGS = "-O3 -march=native -ffp-contract=off -fopenmp -fPIC -std=c++17 -Wall -Wno-unknown-pragmas"
 
 DIRECT_FAST, DIRECT_ONE_ARCTAN, BARNES_HUT = 0, 1, 2
 SEG_BSPLINE, SEG_CATMULLROM, SEG_BEZIER, SEG_POLYLINE = 0, 1, 2, 3
@@ -30,11 +36,38 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        build()
-        L = C.CDLL(_LIB_PATH)
+def native_key() -> str:
+    """A short key of this host's CPU (model name and feature flags)."""
+    import hashlib
+    info = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    info += line
+                if line.strip() == "":
+                    break
+    except OSError:
+        import platform
+        info = platform.processor()
+    return hashlib.sha256(info.encode()).hexdigest()[:12]
+
+
+def build_native() -> str:
+    """Compiles the oracle with the reference's -O3 -march=native for this
+    host's CPU (once per CPU model) and returns the library path."""
+    out = os.path.join("_build", "native-" + native_key())
+    path = os.path.join(_HERE, out, "liboracle.so")
+    if not os.path.exists(path):
+        subprocess.run(["make", "-s", "-C", _HERE, f"OUT={out}", f"CXXFLAGS={_NATIVE_FLAGS}",
+                        os.path.join(out, "liboracle.so")], check=True)
+    return path
+
+
+def lib(native: bool = False):
+    path = build_native() if native else build()
+    if path not in _libs:
+        L = C.CDLL(path)
         vp, i32p, i64p, f64p, u64p = (C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_double), C.POINTER(C.c_uint64))
         L.orc_last_error.restype = C.c_char_p
@@ -63,8 +96,8 @@ def lib():
         L.orc_certificate_text.argtypes = [vp, C.c_char_p]
         L.orc_certificate.restype = C.c_int64
         L.orc_max_threads.restype = C.c_int
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _p(a, t):
@@ -78,8 +111,8 @@ class OracleError(RuntimeError):
 class Oracle:
     """One model in the oracle: load -> prepare (PLS, Discretize, PLS) -> evaluate."""
 
-    def __init__(self):
-        self._L = lib()
+    def __init__(self, native: bool = False):
+        self._L = lib(native)
         self._h = self._L.orc_create()
 
     def __del__(self):
@@ -185,5 +218,5 @@ class Oracle:
         return buf.value.decode(), mean.value, mx.value
 
 
-def max_threads() -> int:
-    return lib().orc_max_threads()
+def max_threads(native: bool = False) -> int:
+    return lib(native).orc_max_threads()

@@ -12,7 +12,7 @@ development container, never on the GPU hosts:
 * ``manifest.json`` — expected mean off-integer errors of the default
   Barnes–Hut run (test.sh:4,14,24,34,45) and the oracle's own values.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference/checkout
 """
 from __future__ import annotations
 
@@ -162,4 +162,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden.py /path/to/reference/checkout")
+    main(sys.argv[1])

@@ -56,6 +56,48 @@ def test_noalloc_matches_allocating_entry_point(prec, tol):
     assert np.count_nonzero(np.round(ref.cpu().numpy())) > 0
 
 
+def test_noalloc_mixed_near_contacts():
+    """Dense knots and walks: many segment pairs lie between one and four
+    segment lengths apart, where the mixed precision's FP64 rule for near
+    terms (near_factor, default 4) decides the result. The allocation-free
+    call must use the same factor as the allocating entry point."""
+    torch = pytest.importorskip("torch")
+    L = N.load()
+    off, xyz = workloads.mixed_batch(seed=9, n_loops=40, hi=2 ** 12, cube=20.0)
+    m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
+    poff, pxyz, pairs, _ = m.Prepare(True)
+    d_xyz = torch.from_numpy(pxyz).cuda()
+    d_off = torch.from_numpy(poff).cuda()
+    d_pairs = torch.from_numpy(pairs).cuda()
+    n, nl = len(pairs), len(poff) - 1
+    eng = Engine(0)
+    ref = {}
+    near = {}
+    for name, prec, factor in (("fp64", N.PREC_FP64, 4.0), ("mixed", N.PREC_MIXED, 4.0),
+                               ("mixed_f1", N.PREC_MIXED, 1.0)):
+        r = torch.zeros(n, dtype=torch.float64, device="cuda")
+        eng.linking_numbers_device(d_xyz.data_ptr(), d_off.data_ptr(), nl, d_pairs.data_ptr(), n, r.data_ptr(),
+                                   method="directsum", precision=prec, fp64_margin=0.0, near_factor=factor)
+        torch.cuda.synchronize()
+        ref[name] = r.cpu().numpy()
+        near[name] = eng.stats()["near_fp64_terms"]
+    # The band between one and four segment lengths is populated.
+    assert near["mixed"] > near["mixed_f1"] > 0
+    for _ in range(2):
+        out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        st = _call(L, d_xyz.data_ptr(), d_off.data_ptr(), nl, d_pairs.data_ptr(), n, N.PREC_MIXED,
+                   out.data_ptr())
+        assert st == 0, L.fln_last_error()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        np.testing.assert_allclose(got, ref["mixed"], rtol=0, atol=1e-5)
+        np.testing.assert_allclose(got, ref["fp64"], rtol=0, atol=1e-5)
+    print(f"near contacts: {n} pairs, FP64 near terms {near['mixed']:.0f} (factor 4) / "
+          f"{near['mixed_f1']:.0f} (factor 1), max |no-alloc - FP64| {np.abs(got - ref['fp64']).max():.3g}, "
+          f"max |factor 1 - FP64| {np.abs(ref['mixed_f1'] - ref['fp64']).max():.3g}")
+
+
 def test_noalloc_rejects_oversize_and_bad_input():
     torch = pytest.importorskip("torch")
     L = N.load()
