@@ -57,6 +57,7 @@ class TuneResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 MLP_PARAMS = 4801  # FLN_MLP_PARAMS
+ABI_VERSION = 3  # FLN_ABI_VERSION: the layout of the structs below
 
 
 class Params(C.Structure):
@@ -66,7 +67,8 @@ class Params(C.Structure):
         ("precision", C.c_int32), ("fp64_margin", C.c_double), ("near_factor", C.c_double),
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
         ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("bh_budget", C.c_int32),
-        ("bh_bucket", C.c_int32),
+        ("bh_bucket", C.c_int32), ("bh_retry_from_roots", C.c_int32), ("bh_spill_cap", C.c_int32),
+        ("bh_wait_polls", C.c_int64), ("reserved_params", C.c_double * 4),
     ]
 
 
@@ -80,11 +82,13 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int32), ("ms_main_kernel", C.c_double),
         ("ms_tree_build", C.c_double), ("bh_rounds", C.c_int32), ("reserved_stats", C.c_int32),
         ("bh_escalated", C.c_int64), ("bh_wait_timeouts", C.c_int64),
-        ("ms_exact", C.c_double), ("bh_exact_entries", C.c_double),
+        ("ms_exact", C.c_double), ("bh_exact_entries", C.c_double), ("ms_retry", C.c_double),
+        ("bh_front_records", C.c_int64), ("bh_retry_from_roots", C.c_int64),
+        ("reserved_stats2", C.c_double * 4),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
 class LearnedOptions(C.Structure):
@@ -136,6 +140,9 @@ def load():
     L.fln_status_string.argtypes = [C.c_int]
     L.fln_last_error.restype = C.c_char_p
     L.fln_abi_version.restype = C.c_int
+    if L.fln_abi_version() != ABI_VERSION:
+        raise FlnError(13, f"{LIB_PATH} has ABI version {L.fln_abi_version()}, this binding expects "
+                           f"{ABI_VERSION}: rebuild it")
     L.fln_default_params.argtypes = [P(Params)]
     L.fln_ctx_create.argtypes = [C.c_int, vp, P(vp)]
     L.fln_ctx_destroy.argtypes = [vp]

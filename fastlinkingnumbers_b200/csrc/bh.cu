@@ -531,6 +531,16 @@ struct Batch {
   int2 pairs[32];
 };
 
+// Frontier of a Barnes–Hut pass: the far node pairs of one loop pair (slot),
+// up to kFrontPairs per record, recorded so that the beta retry can continue
+// from them instead of from the roots.
+constexpr int kFrontPairs = 128;
+struct FrontRec {
+  int32_t slot;
+  int32_t count;
+  int2 pairs[kFrontPairs];
+};
+
 struct TravArgs {
   const double *xyz;
   const int64_t *off;
@@ -556,6 +566,20 @@ struct TravArgs {
   int2 *spill;                 // kSpill per warp
   unsigned long long *queue;   // batch queue head
   int32_t *status;             // nonzero on overflow
+  // Second input source, taken after in[0, nin): frontier records of an
+  // earlier pass (the beta retry's continuation); records of slots with
+  // skip[slot] != 0 are passed over.
+  const FrontRec *in1;
+  int64_t nin1;
+  const uint8_t *skip;
+  // Frontier recording (the kFront instantiations): every far node pair
+  // evaluated goes into a record of its slot; a slot whose records do not
+  // fit gets front_lost[slot] = 1 (its retry then starts from the roots).
+  FrontRec *front;
+  unsigned long long *front_count;
+  int64_t front_cap;
+  uint8_t *front_lost;
+  int32_t spill_cap;           // global spill entries per warp used (<= kSpill)
   // Learned opening criterion (frag == nullptr: off).
   LearnedCfg learned;
   double beta0;
@@ -880,13 +904,52 @@ __device__ __noinline__ void shift_down(int2 *stack, int k, int n, int lane) {
   }
 }
 
+// Appends n (<= 32) far node pairs, one per lane (lanes < n), to the warp's
+// open frontier record of `slot`, reserving records as they fill. The open
+// record is (fr, ffill); fr < 0 means none. A record is closed (its header
+// written) when it is full, when the warp moves to another slot, or when the
+// warp finishes.
+__device__ __forceinline__ void front_close(const TravArgs &A, long long &fr, int &ffill, int slot, int lane) {
+  if (fr >= 0 && lane == 0 && fr < A.front_cap) {
+    A.front[fr].slot = slot;
+    A.front[fr].count = ffill;
+  }
+  fr = -1;
+  ffill = 0;
+}
+__device__ __forceinline__ void front_put(const TravArgs &A, long long &fr, int &ffill, int slot, int2 q, int n,
+                                          int lane) {
+  const int need = (fr < 0 ? 1 : 0) + (ffill + n > kFrontPairs ? 1 : 0);
+  long long c = 0;
+  if (lane == 0 && need) c = (long long)atomicAdd(A.front_count, (unsigned long long)need);
+  c = __shfl_sync(0xffffffffu, c, 0);
+  const long long cur = fr < 0 ? c : fr, nxt = fr < 0 ? c + 1 : c;
+  const int pos = ffill + lane;
+  const long long dst = pos < kFrontPairs ? cur : nxt;
+  if (lane < n && dst < A.front_cap) A.front[dst].pairs[pos < kFrontPairs ? pos : pos - kFrontPairs] = q;
+  if (lane == 0 && (cur >= A.front_cap || (ffill + n > kFrontPairs && nxt >= A.front_cap))) A.front_lost[slot] = 1;
+  if (ffill + n >= kFrontPairs) {
+    long long full = cur;
+    int nfull = kFrontPairs;
+    front_close(A, full, nfull, slot, lane);
+    fr = ffill + n > kFrontPairs ? nxt : -1;
+    ffill = ffill + n - kFrontPairs;
+  } else {
+    fr = cur;
+    ffill += n;
+  }
+}
+
 // One warp per batch. The warp runs the two-tree traversal of its batch's
 // node pairs for at most `budget` steps; whatever is still on its stack then
 // is written out as new batches for the next round, so a heavy loop pair
 // spreads over many warps while light pairs finish in one go.
 // kLearn: the learned opening criterion (A.learned); kRecord: sampling of
-// training node pairs (A.rec). The plain instantiation has neither.
-template <bool kLearn, bool kRecord>
+// training node pairs (A.rec); kFront: frontier recording (A.front). The
+// plain instantiation has none of them.
+// Input: the batches in[0, nin), then the frontier records in1[0, nin1)
+// (up to kFrontPairs node pairs each), taken one at a time from A.queue.
+template <bool kLearn, bool kRecord, bool kFront>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
@@ -907,18 +970,36 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
   int2 *spill = A.spill + (size_t)gw * kSpill;
   double nfar = 0, nent = 0;
+  long long frec = -1;  // open frontier record (kFront)
+  int ffill = 0, fslot = -1;
+  const long long total = A.nin + A.nin1;
   for (;;) {
     long long b = 0;
     if (lane == 0) {
       // Past the soft limit of the exact list this round takes no new batch
       // (they carry over).
       const bool full = (int64_t)*(volatile unsigned long long *)A.bkt_count > A.bkt_soft;
-      b = full ? A.nin : (long long)atomicAdd(A.queue, 1ULL);
+      b = full ? total : (long long)atomicAdd(A.queue, 1ULL);
     }
     b = __shfl_sync(0xffffffffu, b, 0);
-    if (b >= A.nin) break;
-    const int slot = A.in[b].slot;
-    const int cnt0 = A.in[b].count;
+    if (b >= total) break;
+    int slot, cnt0;
+    const int2 *src;
+    if (b < A.nin) {
+      slot = A.in[b].slot;
+      cnt0 = A.in[b].count;
+      src = A.in[b].pairs;
+    } else {
+      const FrontRec &r = A.in1[b - A.nin];
+      slot = r.slot;
+      cnt0 = r.count;
+      src = r.pairs;
+      if (cnt0 <= 0 || A.skip[slot]) continue;
+    }
+    if constexpr (kFront) {
+      if (slot != fslot) front_close(A, frec, ffill, fslot, lane);
+      fslot = slot;
+    }
     const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
     const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
@@ -926,7 +1007,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     const double itolsq = A.itolsq[slot], eps = A.epssq;
     // Threshold of the learned criterion: tau x (beta0 / beta)^4 in later passes.
     const float log10_tau = A.learned.log10_tau + 2.f * (float)log10(A.beta0 * A.beta0 / itolsq);
-    if (lane < cnt0) stack[lane] = A.in[b].pairs[lane];
+    for (int x = lane; x < cnt0; x += 32) stack[x] = src[x];
     int top = cnt0, nspill = 0, nf = 0, steps = 0;
     long long bc = -1;  // open chunk of the exact list
     int bfill = 0;      // entries in it
@@ -1048,7 +1129,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       const int ns = __popc(sm);
       if (top + 2 * ns > kStack) {  // spill the oldest half
         const int k = top / 2;
-        if (nspill + k > kSpill) {
+        if (nspill + k > A.spill_cap) {
           overflow = true;
           break;
         }
@@ -1120,6 +1201,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         const int2 q = farq[nf - 32 + lane];
         const float4 v = farv[nf - 32 + lane];
         const float2 rr = farr[nf - 32 + lane];
+        if constexpr (kFront) front_put(A, frec, ffill, slot, q, 32, lane);
         far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)v.w, rr.x, rr.y, sum, err);
         nfar += 32;
         nf -= 32;
@@ -1127,6 +1209,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       }
     }
     // Evaluate what is still queued.
+    if constexpr (kFront) {
+      if (nf > 0) front_put(A, frec, ffill, slot, lane < nf ? farq[lane] : make_int2(0, 0), nf, lane);
+    }
     if (lane < nf) {
       const int2 q = farq[lane];
       const float4 v = farv[lane];
@@ -1149,6 +1234,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       fix_add(A.acc_err + slot, err);
     }
   }
+  if constexpr (kFront) front_close(A, frec, ffill, fslot, lane);
   if (lane == 0) {
     atomicAdd(A.counts, nfar);
     atomicAdd(A.counts + 5, nent);
@@ -1281,14 +1367,17 @@ __global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArg
   if (lane == 0 && nexact > 0) atomicAdd(A.counts + 1, nexact);
 }
 
-#ifdef FLN_BH_MIN_CTAS
-__global__ void __launch_bounds__(32 * kWarps, FLN_BH_MIN_CTAS) bh_traverse(TravArgs A) { traverse<false, false>(A); }
-#else
-__global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { traverse<false, false>(A); }
-#endif
-__global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true>(A); }
-// Four CTAs per SM, as the plain kernel gets with its natural register count.
-__global__ void __launch_bounds__(32 * kWarps, 3) bh_traverse_learned(TravArgs A) { traverse<true, false>(A); }
+// (Without a minimum CTA count: ptxas then settles at 96 registers, five CTAs
+// per SM; a minimum of 1 let it take 138.)
+__global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { traverse<false, false, false>(A); }
+// The first pass, which records its frontier for the beta retry.
+__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_front(TravArgs A) { traverse<false, false, true>(A); }
+__global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, false>(A); }
+// Three CTAs per SM (168 registers).
+__global__ void __launch_bounds__(32 * kWarps, 3) bh_traverse_learned(TravArgs A) { traverse<true, false, false>(A); }
+__global__ void __launch_bounds__(32 * kWarps, 3) bh_traverse_learned_front(TravArgs A) {
+  traverse<true, false, true>(A);
+}
 
 // ------------------------------------------------------------------ split evaluation
 // Rounds with the evaluation taken out of the traversal: bh_classify walks
@@ -1544,9 +1633,11 @@ __global__ void __launch_bounds__(256) bh_leaf_chunks(EvalArgs A) {
 }
 
 // Initial batches: the root pair of every slot in `slots`; clears their sums.
+// The root pair of each listed slot as a batch; clears the slot's far,
+// exact and error sums.
 __global__ void root_batches(const int32_t *slots, int64_t n, const int32_t *slot_loops, const int64_t *off,
                              int32_t tree_kind, Batch *out, unsigned long long *acc_lk,
-                             unsigned long long *acc_err) {
+                             unsigned long long *acc_err, unsigned long long *acc_exact) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int s = slots[k];
@@ -1558,15 +1649,27 @@ __global__ void root_batches(const int32_t *slots, int64_t n, const int32_t *slo
                                    : make_int2((int)(n1 - 2), (int)(n2 - 2));
   acc_lk[s] = 0;
   acc_err[s] = 0;
+  acc_exact[s] = 0;
 }
 
-// Fixed-point sums -> per caller pair doubles.
+// Slots whose beta retry continues from the first pass's frontier: the far
+// and error sums restart, the exact sum of the first pass stays.
+__global__ void continue_slots(const int32_t *slots, int64_t n, unsigned long long *acc_lk,
+                               unsigned long long *acc_err) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  acc_lk[slots[k]] = 0;
+  acc_err[slots[k]] = 0;
+}
+
+// Fixed-point sums (far-field + exact) -> per caller pair doubles.
 __global__ void finish_sums(const unsigned long long *acc_lk, const unsigned long long *acc_err,
-                            const int32_t *slot_pair, int64_t nslots, double *lk, double *err) {
+                            const unsigned long long *acc_exact, const int32_t *slot_pair, int64_t nslots,
+                            double *lk, double *err) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots) return;
   const int p = slot_pair[s];
-  lk[p] = (double)(long long)acc_lk[s] / kFix;
+  lk[p] = (double)(long long)(acc_lk[s] + acc_exact[s]) / kFix;
   err[p] = (double)(long long)acc_err[s] / kFix;
 }
 
@@ -1610,6 +1713,8 @@ struct PersistArgs {
   double *counts;              // [0] far, [1] leaf, [2] retried, [3] escalated
   int2 *spill;
   int32_t *status;
+  int32_t spill_cap;           // global spill entries per warp used (<= kSpill)
+  long long wait_polls;        // polls before a wait gives up (status bit 1)
 };
 
 __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long *p) {
@@ -1742,7 +1847,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
             slot = -2;  // all work done
             break;
           }
-          if (++polls > kWaitPolls) {
+          if (++polls > A.wait_polls) {
             atomicOr(A.status, 2);
             slot = -2;
             break;
@@ -1863,7 +1968,7 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
       const int ns = __popc(sm);
       if (top + 2 * ns > kStack) {
         const int k = top / 2;
-        if (nspill + k > kSpill) {
+        if (nspill + k > A.spill_cap) {
           overflow = true;
           break;
         }
@@ -2238,15 +2343,22 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   double *d_itol = ctx.d_bh[12].as<double>(np);
   double *d_counts = ctx.d_bh[13].as<double>(8);  // far, leaf, retried, escalated, status words
   int32_t *d_status = reinterpret_cast<int32_t *>(d_counts + 2);
-  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(2 * np + 8);
+  // Per slot, fixed point: far-field sum, error estimate, exact sum.
+  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(3 * np + 8);
   unsigned long long *d_acc_err = d_acc + np;
-  unsigned long long *d_ctr = d_acc + 2 * np;  // [0] queue, [1] next-round count, [2] far chunks, [3] leaf chunks
-  int per_sm = 0;
+  unsigned long long *d_acc_exact = d_acc + 2 * np;
+  // [0] queue, [1] next-round count, [2] exact (or far) chunks, [3] leaf chunks, [4] frontier records
+  unsigned long long *d_ctr = d_acc + 3 * np;
+  int per_sm = 0, per_sm_f = 0;
   FLN_CUDA(cudaFuncSetAttribute(bh_traverse, cudaFuncAttributePreferredSharedMemoryCarveout, FLN_BH_CARVEOUT));
+  FLN_CUDA(cudaFuncSetAttribute(bh_traverse_front, cudaFuncAttributePreferredSharedMemoryCarveout, FLN_BH_CARVEOUT));
   FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_traverse, 32 * kWarps, 0));
+  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, bh_traverse_front, 32 * kWarps, 0));
   per_sm = std::max(per_sm, 1);
   const int grid = ctx.num_sms * per_sm;
+  const int grid_f = ctx.num_sms * std::max(std::min(per_sm_f, per_sm), 1);
   const int64_t nwarps = (int64_t)grid * kWarps;
+  const int spill_cap = prm.bh_spill_cap > 0 ? std::min(prm.bh_spill_cap, kSpill) : kSpill;
   int per_sm_l = 0;
   FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, bh_traverse_learned, 32 * kWarps, 0));
   const int grid_l = ctx.num_sms * std::max(per_sm_l, 1);  // <= grid: the learned kernel uses more registers
@@ -2286,18 +2398,46 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     d_leaf = reinterpret_cast<Chunk *>(ctx.d_bh[17].need((size_t)chunk_cap * sizeof(Chunk)));
   }
   ctx.stats.bh_rounds = 0;
-  // One Barnes–Hut pass over the slots in `active` with per-slot beta^2.
-  auto pass = [&](const std::vector<int32_t> &active, const std::vector<double> &itol_slots, bool record) {
-    const int64_t na = (int64_t)active.size();
-    FLN_CUDA(cudaMemcpyAsync(d_active, active.data(), na * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  // Frontier of the first pass (bh_schedule 0): its far node pairs, so that
+  // the beta retry continues from them. Sized from the previous call's
+  // frontier (grow-only); slots whose records do not fit retry from the roots.
+  const bool use_front = prm.bh_schedule == 0 && !prm.bh_retry_from_roots && !ctx.recording.rec;
+  FrontRec *d_front = nullptr;
+  uint8_t *d_lost = nullptr, *d_skip = nullptr;
+  int64_t front_cap = 0;
+  if (use_front) {
+    size_t free_b = 0, total_b = 0;
+    FLN_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t have = ctx.d_bh[23].bytes / sizeof(FrontRec);
+    size_t want = ctx.bh_front_hint > 0 ? (size_t)(1.25 * (double)ctx.bh_front_hint) + 1024
+                                        : std::min<size_t>((size_t)16 << 30, free_b / 5) / sizeof(FrontRec);
+    want = std::max(want, have);
+    if (want > have && (want - have) * sizeof(FrontRec) > free_b / 2) want = have + free_b / 2 / sizeof(FrontRec);
+    front_cap = (int64_t)std::max<size_t>(want, 1024);
+    d_front = reinterpret_cast<FrontRec *>(ctx.d_bh[23].need((size_t)front_cap * sizeof(FrontRec)));
+    d_lost = ctx.d_bh[25].as<uint8_t>(2 * np);
+    d_skip = d_lost + np;
+    FLN_CUDA(cudaMemsetAsync(d_lost, 0, np, st));
+  }
+  int64_t front_n = 0;  // records the first pass wrote (<= front_cap)
+  // One Barnes–Hut pass with per-slot beta^2: the root pairs of the slots in
+  // `roots`, then (the retry's continuation) the frontier records of the
+  // slots whose skip byte is 0. `front` records this pass's frontier.
+  auto pass = [&](const std::vector<int32_t> &roots, const std::vector<double> &itol_slots, bool record, bool front,
+                  int64_t nstream) {
+    const int64_t na = (int64_t)roots.size();
+    FLN_CUDA(cudaMemcpyAsync(d_active, roots.data(), na * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     FLN_CUDA(cudaMemcpyAsync(d_itol, itol_slots.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
-    root_batches<<<(int)((na + 255) / 256), 256, 0, st>>>(d_active, na, d_slots, d_off, prm.bh_tree == 1 ? 1 : 0,
-                                                          d_batch[0], d_acc, d_acc_err);
-    FLN_CUDA(cudaGetLastError());
-    ++launches;
-    int64_t nin = na;
+    if (na > 0) {
+      root_batches<<<(int)((na + 255) / 256), 256, 0, st>>>(d_active, na, d_slots, d_off, prm.bh_tree == 1 ? 1 : 0,
+                                                            d_batch[0], d_acc, d_acc_err, d_acc_exact);
+      FLN_CUDA(cudaGetLastError());
+      ++launches;
+    }
+    if (front) FLN_CUDA(cudaMemsetAsync(d_ctr + 4, 0, sizeof(unsigned long long), st));
+    int64_t nin = na, pos = 0;
     int cur = 0;
-    for (int round = 0; nin > 0 && round < 4096; ++round) {
+    for (int round = 0; (nin > 0 || pos < nstream) && round < 65536; ++round) {
       FLN_CUDA(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
       if (prm.bh_schedule == 2) {
         // Classify, then evaluate this round's chunks.
@@ -2337,7 +2477,10 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       }
       TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
                  d_batch[1 - cur], cap, d_ctr + 1, budget, bucket, d_bkt, d_ctr + 2, bkt_soft, bkt_cap, d_acc,
-                 d_acc_err, d_counts, d_spill, d_ctr, d_status, ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
+                 d_acc_err, d_counts, d_spill, d_ctr, d_status,
+                 d_front + pos, nstream - pos, d_skip,
+                 front ? d_front : nullptr, d_ctr + 4, front_cap, d_lost, spill_cap,
+                 ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
       if (record) {
         A.rec = ctx.recording.rec;
         A.rec_count = ctx.recording.count;
@@ -2345,16 +2488,17 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         A.rec_smin = ctx.recording.s_min;
         A.rec_keep = ctx.recording.keep;
       }
-      const int gmax = (A.learned.frag && !A.rec) ? grid_l : grid;
-      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, gmax));
+      const int gmax = (A.learned.frag && !A.rec) ? grid_l : (front ? grid_f : grid);
+      const int64_t work = nin + (nstream - pos);
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((work + kWarps - 1) / kWarps, gmax));
       if (A.rec)
         bh_traverse_record<<<g, 32 * kWarps, 0, st>>>(A);
       else if (A.learned.frag)
-        bh_traverse_learned<<<g, 32 * kWarps, 0, st>>>(A);
+        (front ? bh_traverse_learned_front : bh_traverse_learned)<<<g, 32 * kWarps, 0, st>>>(A);
       else
-        bh_traverse<<<g, 32 * kWarps, 0, st>>>(A);
+        (front ? bh_traverse_front : bh_traverse)<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
-      BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc, d_counts};
+      BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc_exact, d_counts};
       FLN_CUDA(cudaEventRecord(ctx.ev_bk[0], st));
       bh_buckets<<<ctx.num_sms * 8, 256, 0, st>>>(BA);
       FLN_CUDA(cudaGetLastError());
@@ -2365,18 +2509,30 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       FLN_CUDA(cudaMemcpyAsync(c2, d_ctr, sizeof c2, cudaMemcpyDeviceToHost, st));
       FLN_CUDA(cudaStreamSynchronize(st));
       ctx.stats.ms_exact += ctx.elapsed(ctx.ev_bk[0], ctx.ev_bk[1]);
-      // Batches not taken this round (past the soft limit) carry over.
+      // Input not taken this round (past the soft limit) carries over: the
+      // batches by copy, the frontier records by position.
       int64_t next = (int64_t)std::min<unsigned long long>(c2[1], (unsigned long long)cap);
-      const int64_t taken = (int64_t)std::min<unsigned long long>(c2[0], (unsigned long long)nin);
+      const int64_t taken = (int64_t)std::min<unsigned long long>(c2[0], (unsigned long long)(nin + nstream - pos));
       if (taken < nin) {
         const int64_t keep = std::min<int64_t>(nin - taken, cap - next);
         FLN_CUDA(cudaMemcpyAsync(d_batch[1 - cur] + next, d_batch[cur] + taken, keep * sizeof(Batch),
                                  cudaMemcpyDeviceToDevice, st));
         if (keep < nin - taken) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut round buffer too small");
         next += keep;
+      } else {
+        pos += taken - nin;
       }
       nin = next;
       cur = 1 - cur;
+    }
+    if (nin > 0 || pos < nstream) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut pass did not finish in 65536 rounds");
+    if (front) {
+      unsigned long long nrec = 0;
+      FLN_CUDA(cudaMemcpyAsync(&nrec, d_ctr + 4, sizeof nrec, cudaMemcpyDeviceToHost, st));
+      FLN_CUDA(cudaStreamSynchronize(st));
+      front_n = (int64_t)std::min<unsigned long long>(nrec, (unsigned long long)front_cap);
+      ctx.bh_front_hint = std::max<int64_t>(ctx.bh_front_hint, (int64_t)nrec);
+      ctx.stats.bh_front_records = (int64_t)nrec;
     }
   };
   // bh_schedule = 1: one persistent launch (retry and escalation on the
@@ -2408,7 +2564,8 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     PersistArgs P{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_slot_pair, (int32_t)np, prm.bh_tree == 1 ? 1 : 0,
                   prm.epssq, b0, prm.barnes_hut_beta_limit, prm.target_error, prm.error_est_scale,
                   prm.bh_err_limit, prm.bh_escalations, d_sitol, d_pass_arr, d_left, d_acc, d_acc_err, d_ring,
-                  d_ready, d_q, d_lk_out, d_err_out, d_fl, d_cnt4, d_spill, d_status};
+                  d_ready, d_q, d_lk_out, d_err_out, d_fl, d_cnt4, d_spill, d_status, spill_cap,
+                  prm.bh_wait_polls > 0 ? (long long)prm.bh_wait_polls : kWaitPolls};
     int per_sm_p = 0;
     FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, bh_persistent, 32 * kWarps, 0));
     const int gp = std::min(grid, ctx.num_sms * std::max(per_sm_p, 1));
@@ -2444,9 +2601,10 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   std::iota(all.begin(), all.end(), 0);
   std::vector<double> itol(np, b0 * b0);
   FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-  pass(all, itol, ctx.recording.rec != nullptr);
+  pass(all, itol, ctx.recording.rec != nullptr, use_front, 0);
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
-  finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
+  finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_acc_exact, d_slot_pair, np, d_lk_out,
+                                                       d_err_out);
   FLN_CUDA(cudaGetLastError());
   ++launches;
   // Error estimate and beta retry (lnc.cpp:165-184).
@@ -2454,6 +2612,11 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(err.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
   int32_t status = 0;
   FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
+  std::vector<uint8_t> lost;
+  if (use_front) {
+    lost.resize(np);
+    FLN_CUDA(cudaMemcpyAsync(lost.data(), d_lost, np, cudaMemcpyDeviceToHost, st));
+  }
   FLN_CUDA(cudaStreamSynchronize(st));
   ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
   std::vector<int32_t> flags(np, 0), retry_slots;
@@ -2474,9 +2637,41 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   std::vector<double> far_leaf(6, 0.0);
   if (!retry_slots.empty()) {
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-    pass(retry_slots, itol, false);
+    if (use_front && (status & 1) == 0) {
+      // A node pair opened at beta0 is opened at beta* > beta0 (far at beta*
+      // implies far at beta0), and an exact pair stays exact (the bucket test
+      // does not depend on beta). So the beta* pass is the beta0 pass
+      // continued from its far node pairs: the exact sums stay, the far sums
+      // restart from the frontier. Slots whose frontier did not fit start
+      // from the roots.
+      std::vector<uint8_t> skip(np, 1);
+      std::vector<int32_t> cont, from_roots;
+      for (int32_t sl : retry_slots) {
+        if (lost[sl]) {
+          from_roots.push_back(sl);
+        } else {
+          cont.push_back(sl);
+          skip[sl] = 0;
+        }
+      }
+      FLN_CUDA(cudaMemcpyAsync(d_skip, skip.data(), np, cudaMemcpyHostToDevice, st));
+      if (!cont.empty()) {
+        int32_t *d_cont = reinterpret_cast<int32_t *>(ctx.d_bh[24].need(cont.size() * sizeof(int32_t)));
+        FLN_CUDA(cudaMemcpyAsync(d_cont, cont.data(), cont.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        continue_slots<<<(int)((cont.size() + 255) / 256), 256, 0, st>>>(d_cont, (int64_t)cont.size(), d_acc,
+                                                                           d_acc_err);
+        FLN_CUDA(cudaGetLastError());
+        ++launches;
+      }
+      ctx.stats.bh_retry_from_roots = (int64_t)from_roots.size();
+      pass(from_roots, itol, false, false, cont.empty() ? 0 : front_n);
+    } else {
+      ctx.stats.bh_retry_from_roots = (int64_t)retry_slots.size();
+      pass(retry_slots, itol, false, false, 0);
+    }
     FLN_CUDA(cudaEventRecord(ctx.ev3, st));
-    finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
+    finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_acc_exact, d_slot_pair, np, d_lk_out,
+                                                         d_err_out);
     FLN_CUDA(cudaGetLastError());
     ++launches;
     // The reported estimate is that of the final run, scaled like the first
@@ -2486,7 +2681,9 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     FLN_CUDA(cudaMemcpyAsync(e2.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
     FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
     FLN_CUDA(cudaStreamSynchronize(st));
-    ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+    const double ms = ctx.elapsed(ctx.ev2, ctx.ev3);
+    ctx.stats.ms_main_kernel += ms;
+    ctx.stats.ms_retry += ms;
     for (int64_t p = 0; p < np; ++p)
       if (retried[p]) err[p] = e2[p] * prm.error_est_scale;
   }
@@ -2509,16 +2706,19 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     if (up.empty()) break;
     ctx.stats.bh_escalated += (int64_t)up.size();
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
-    pass(up, itol, false);
+    pass(up, itol, false, false, 0);
     FLN_CUDA(cudaEventRecord(ctx.ev3, st));
-    finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_slot_pair, np, d_lk_out, d_err_out);
+    finish_sums<<<(int)((np + 255) / 256), 256, 0, st>>>(d_acc, d_acc_err, d_acc_exact, d_slot_pair, np, d_lk_out,
+                                                         d_err_out);
     FLN_CUDA(cudaGetLastError());
     ++launches;
     std::vector<double> e3(np);
     FLN_CUDA(cudaMemcpyAsync(e3.data(), d_err_out, np * sizeof(double), cudaMemcpyDeviceToHost, st));
     FLN_CUDA(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
     FLN_CUDA(cudaStreamSynchronize(st));
-    ctx.stats.ms_main_kernel += ctx.elapsed(ctx.ev2, ctx.ev3);
+    const double ms = ctx.elapsed(ctx.ev2, ctx.ev3);
+    ctx.stats.ms_main_kernel += ms;
+    ctx.stats.ms_retry += ms;
     for (int32_t s : up) err[order[s]] = e3[order[s]] * prm.error_est_scale;
   }
   FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));

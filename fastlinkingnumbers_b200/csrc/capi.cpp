@@ -142,6 +142,9 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   ctx.stats.ms_tree_build = 0;
   ctx.stats.bh_far_evals = ctx.stats.bh_leaf_evals = 0;
   ctx.stats.ms_exact = ctx.stats.bh_exact_entries = 0;
+  ctx.stats.ms_retry = 0;
+  ctx.stats.bh_front_records = ctx.stats.bh_retry_from_roots = 0;
+  ctx.stats.bh_wait_timeouts = 0;
   ctx.stats.beta_retried = 0;
   ctx.stats.bh_escalated = 0;
   if (!d_err) d_err = ctx.d_err.as<double>(std::max<int64_t>(np, 1));  // Barnes–Hut needs one
@@ -228,6 +231,10 @@ static fln_params resolved(const fln_params *p) {
   if (r.bh_budget != 0 && (r.bh_budget < 16 || r.bh_budget > 4096))
     throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_budget 0 or in [16, 4096]");
   if (r.bh_bucket < 0 || r.bh_bucket > 16) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_bucket in [0, 16]");
+  if (r.bh_retry_from_roots != 0 && r.bh_retry_from_roots != 1)
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_retry_from_roots is 0 or 1");
+  if (r.bh_spill_cap < 0 || r.bh_spill_cap > 8192) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_spill_cap in [0, 8192]");
+  if (r.bh_wait_polls < 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_wait_polls must not be negative");
   return r;
 }
 

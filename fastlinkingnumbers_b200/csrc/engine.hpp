@@ -103,7 +103,8 @@ struct Context {
   fln_stats stats{};
   // Device buffers.
   DevBuf d_xyz, d_off, d_pairs, d_loops, d_items, d_partial, d_counter, d_lk, d_err, d_flags, d_near;
-  DevBuf d_bh[24];
+  DevBuf d_bh[28];
+  int64_t bh_front_hint = 0;  // frontier records of the largest Barnes–Hut first pass so far
   HostBuf h_in, h_out;  // pinned staging of copy_h2d / copy_d2h
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   cudaEvent_t ev_bk[2] = {nullptr, nullptr};  // around each exact-list launch

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define FLN_ABI_VERSION 2
+#define FLN_ABI_VERSION 3
 
 typedef enum fln_status {
   FLN_OK = 0,
@@ -95,6 +95,19 @@ typedef struct fln_params {
                                    leaf pair and has at most this many segments a side is summed exactly,
                                    segment pair by segment pair; 0 = 8, 1 = leaf pairs only (the
                                    reference's traversal), at most 16 */
+  int32_t bh_retry_from_roots;  /* 0 (default): bh_schedule 0 continues the beta retry from the first pass's
+                                   far node pairs (a node pair opened at beta0 is opened at the larger beta,
+                                   an exact one stays exact, so the node pairs and the sums are those of a
+                                   run from the roots); 1: the retry re-runs from the roots, as
+                                   lnc.cpp:165-184 does */
+  int32_t bh_spill_cap;         /* global spill entries per warp of the traversal stacks; 0 = 8192, the
+                                   maximum. A traversal that needs more fails with FLN_ERR_STACK_OVERFLOW
+                                   (bh_schedule 0 and 1); smaller values exist to test that bound */
+  int64_t bh_wait_polls;        /* bh_schedule 1: polls (with a nanosleep back-off of up to 2 us) before
+                                   a waiting warp gives up, after which the stage reruns with budgeted
+                                   rounds (fln_stats.bh_wait_timeouts); 0 = 2^21, a few seconds; smaller
+                                   values exist to test that path */
+  double reserved_params[4];    /* zero */
 } fln_params;
 
 /* Statistics of the last computation on a context. */
@@ -123,6 +136,13 @@ typedef struct fln_stats {
   double ms_exact;              /* Barnes–Hut: device time of the exact-list kernel (part of ms_main_kernel) */
   double bh_exact_entries;      /* Barnes–Hut: node pairs summed exactly (leaf pairs and small node pairs);
                                    bh_leaf_evals counts their segment pairs */
+  double ms_retry;              /* Barnes–Hut: device time of the beta retry and escalation passes (part of
+                                   ms_main_kernel) */
+  int64_t bh_front_records;     /* Barnes–Hut: frontier records (up to 128 far node pairs each) written by
+                                   the first pass for the retry to continue from */
+  int64_t bh_retry_from_roots;  /* Barnes–Hut: retried pairs that restarted from the roots (frontier not
+                                   kept for them, or bh_retry_from_roots set) */
+  double reserved_stats2[4];
 } fln_stats;
 
 typedef struct fln_ctx fln_ctx;

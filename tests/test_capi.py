@@ -31,7 +31,7 @@ def test_exports_every_declared_symbol():
 
 def test_status_strings_and_defaults():
     L = N.load()
-    assert L.fln_abi_version() == 2
+    assert L.fln_abi_version() == 3
     assert L.fln_status_string(0) == b"ok"
     p = N.default_params()
     assert (p.barnes_hut_init_beta, p.barnes_hut_beta_limit, p.epssq) == (2.0, 10.0, 1e-24)
