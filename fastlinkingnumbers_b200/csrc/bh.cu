@@ -1001,7 +1001,6 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       fslot = slot;
     }
     const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
-    const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
     const NodeHdr *H1 = A.hdr + A.node_base[l1], *H2 = A.hdr + A.node_base[l2];
     const NodeMom *M1 = A.mom + A.node_base[l1], *M2 = A.mom + A.node_base[l2];
     const double itolsq = A.itolsq[slot], eps = A.epssq;
@@ -1241,19 +1240,22 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
 }
 
-// Exact node pairs of a round: one warp per chunk. Entry j of a chunk is a
-// block of cnt1 x cnt2 segment pairs, cut into runs of up to kRun
-// consecutive segments of loop 2 against one segment of loop 1. The runs are
-// numbered entry by entry and walked 32 at a time, one run per lane, so a
-// warp stays full whatever the entry sizes. Segment pairs left to FP64 (a
-// few percent) wait in a per-warp queue and are evaluated 32 at a time, so
-// that path runs with full warps too. Sums go to the chunk's loop pair in
-// fixed point.
-#ifndef FLN_BUCKET_RUN
-#define FLN_BUCKET_RUN 4
-#endif
-constexpr int kRun = FLN_BUCKET_RUN;
-
+// Exact node pairs of a round: one warp per chunk (up to 32 entries of one
+// loop pair). Entry j is a block of cnt1 x cnt2 segment pairs: segments
+// [lo1, lo1 + cnt1) of loop 1 against [lo2, lo2 + cnt2) of loop 2.
+//
+// Per entry, an FP64 origin o_j (midway between vertex lo1 of loop 1 and
+// vertex lo2 of loop 2) and the entry's cnt2 + 1 loop-2 vertices, relative to
+// o_j and rounded to FP32, are staged in shared memory once (the lane of the
+// entry writes them; .w holds the squared length of the loop-2 segment that
+// starts there). The work is then cut into rows: one loop-1 segment against
+// all cnt2 loop-2 segments of its entry. A lane takes a row, forms its two
+// loop-1 vertices relative to o_j (FP64 difference, rounded once) and walks
+// the staged loop-2 vertices in the vertex form of the reference's direct sum
+// (walk_step_f). Rows are handed out in order of their length, so the lanes
+// of a pass walk about as far. Segment pairs left to FP64 (closer than the
+// longer segment's length) wait in a per-warp queue and are evaluated 32 at
+// a time with full warps. Sums go to the chunk's loop pair in fixed point.
 struct BucketArgs {
   const double *xyz;
   const int64_t *off;
@@ -1261,97 +1263,224 @@ struct BucketArgs {
   const BucketChunk *chunks;
   const unsigned long long *count;
   int64_t cap;
-  unsigned long long *acc_lk;
-  double *counts;  // [1] segment pairs summed exactly
+  unsigned long long *acc_lk;  // per slot: the exact sums
+  double *counts;              // [1] segment pairs summed exactly
 };
 
+constexpr int kBkWarps = 4;     // warps per CTA
+constexpr int kStageV = 320;    // staged loop-2 vertices per warp (32 entries of up to 9, or 16 of up to 17)
+
+struct SegWalkF {        // the carried state of a walk along loop 2 (FP32)
+  float ax, ay, az;      // a = q_k - p0
+  float bx, by, bz;      // b = q_k - p1
+  float aa, bb, ab;      // |a|^2, |b|^2, a.b
+  float la, lb;          // |a|, |b|
+};
+
+__device__ __forceinline__ SegWalkF walk_start_f(float p0x, float p0y, float p0z, float4 q0, float ex, float ey,
+                                                 float ez) {
+  SegWalkF w;
+  w.ax = q0.x - p0x;
+  w.ay = q0.y - p0y;
+  w.az = q0.z - p0z;
+  w.bx = w.ax - ex;
+  w.by = w.ay - ey;
+  w.bz = w.az - ez;
+  w.aa = dot3(w.ax, w.ay, w.az, w.ax, w.ay, w.az);
+  w.bb = dot3(w.bx, w.by, w.bz, w.bx, w.by, w.bz);
+  w.ab = dot3(w.ax, w.ay, w.az, w.bx, w.by, w.bz);
+  w.la = norm_of(w.aa);
+  w.lb = norm_of(w.bb);
+  return w;
+}
+
+// One step q0 -> q1 of the walk (q1.w unused; ff = |q1 - q0|^2 comes from
+// the staged vertex q0): the same terms, the same near rule and the same
+// branch handling as walk_step, from FP32 coordinates relative to an origin.
+__device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, float p0z, float4 q1, float ff,
+                                            float ex, float ey, float ez, float ee, float &acc, float &turns) {
+  const float dx = q1.x - p0x, dy = q1.y - p0y, dz = q1.z - p0z;
+  const float fx = dx - w.ax, fy = dy - w.ay, fz = dz - w.az;
+  const float cx = dx - ex, cy = dy - ey, cz = dz - ez;
+  const float cc = dot3(cx, cy, cz, cx, cy, cz), dd = dot3(dx, dy, dz, dx, dy, dz);
+  const float cd = dot3(cx, cy, cz, dx, dy, dz);
+  const float lc = norm_of(cc), ld = norm_of(dd);
+  const bool near = fminf(fminf(w.aa, w.bb), fminf(cc, dd)) <= fmaxf(ee, ff);
+  if (!near) {
+    const float ca = dot3(cx, cy, cz, w.ax, w.ay, w.az), cb = dot3(cx, cy, cz, w.bx, w.by, w.bz);
+    const float ad = dot3(w.ax, w.ay, w.az, dx, dy, dz);
+    const float det = w.ax * (fy * ez - fz * ey) + w.ay * (fz * ex - fx * ez) + w.az * (fx * ey - fy * ex);
+    const float t = w.la * lc;
+    const float div1 = t * w.lb + w.ab * lc + ca * w.lb + cb * w.la;
+    const float div2 = t * ld + ad * lc + ca * ld + cd * w.la;
+    const float x = div1 * div2 - det * det;
+    const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
+    const float y = det * s;
+    float term;
+    if (s > 0.f && fabsf(y) < 0.25f * x) {
+      term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
+    } else {
+      term = atan2f(y, x);
+      const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
+      if ((s < 0.f) || ((s == 0.f) && (det < 0.f))) turns += sg;
+    }
+    acc += term;
+  }
+  w.ax = dx; w.ay = dy; w.az = dz;
+  w.bx = cx; w.by = cy; w.bz = cz;
+  w.aa = dd; w.bb = cc; w.ab = cd;
+  w.la = ld; w.lb = lc;
+  return !near;
+}
+
 #ifndef FLN_BUCKET_MIN_CTAS
-#define FLN_BUCKET_MIN_CTAS 3
+#define FLN_BUCKET_MIN_CTAS 6
 #endif
-__global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArgs A) {
-  __shared__ int2 s_near[8][64];  // (segment of loop 1, segment of loop 2) per warp
-  const int lane = threadIdx.x & 31;
-  int2 *nq = s_near[threadIdx.x >> 5];
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+__global__ void __launch_bounds__(32 * kBkWarps, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArgs A) {
+  __shared__ float4 s_q[kBkWarps][kStageV];   // staged loop-2 vertices (x, y, z relative to o_j; |segment|^2)
+  __shared__ double s_org[kBkWarps][3][32];   // per entry origin o_j (FP64)
+  __shared__ int2 s_near[kBkWarps][64];       // (segment of loop 1, segment of loop 2) left to FP64
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  float4 *sq = s_q[wi];
+  double(*org)[32] = s_org[wi];
+  int2 *nq = s_near[wi];
+  const int64_t nw = (int64_t)gridDim.x * kBkWarps;
   const int64_t n = min((int64_t)*A.count, A.cap);
+  const unsigned lt = (1u << lane) - 1;
   double nexact = 0;
-  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += nw) {
+  for (int64_t c = (int64_t)blockIdx.x * kBkWarps + wi; c < n; c += nw) {
     const int slot = A.chunks[c].slot, cnt = A.chunks[c].count;
     const int l1 = A.slot_loops[2 * slot], l2 = A.slot_loops[2 * slot + 1];
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1, o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
-    int4 e = make_int4(0, 0, 0, 1);
-    if (lane < cnt) e = A.chunks[c].e[lane];
-    const int nruns = (e.w + kRun - 1) / kRun;   // runs per row
-    const int ni = lane < cnt ? e.z * nruns : 0;  // runs of the entry
-    int incl = ni, pairs = lane < cnt ? e.z * e.w : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-      pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
-    }
-    const int excl = incl - ni;
-    const int items = __shfl_sync(0xffffffffu, incl, 31);
     const double *P1 = A.xyz + 3 * o1, *Q2 = A.xyz + 3 * o2;
+    int4 e = make_int4(0, 0, 0, 0);
+    if (lane < cnt) e = A.chunks[c].e[lane];
+    nexact += (double)__reduce_add_sync(0xffffffffu, (unsigned)(e.z * e.w));
+    // All entries fit the staging area unless bh_bucket > 8 makes them
+    // longer; then the chunk goes in two halves of 16 entries.
+    const int tot = __reduce_add_sync(0xffffffffu, lane < cnt ? e.w + 1 : 0);
+    const int halves = tot > kStageV ? 2 : 1;
     double sum = 0.0;
     int nn = 0;  // queued FP64 pairs
-    for (int base = 0; base < items; base += 32) {
-      const int g = base + lane;
-      // the last entry starting at or before run g (entries past cnt start at items)
-      int j = 0;
+    for (int h = 0; h < halves; ++h) {
+      const bool mine = lane < cnt && (halves == 1 || (lane >> 4) == h);
+      // Staging: lane j writes entry j's origin and loop-2 vertices.
+      const int nv = mine ? e.w + 1 : 0;
+      int vb = nv;
 #pragma unroll
-      for (int st = 16; st; st >>= 1) {
-        const int x = __shfl_sync(0xffffffffu, excl, j + st);
-        if (x <= g) j += st;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, vb, o);
+        if (lane >= o) vb += y;
       }
-      const int lo1 = __shfl_sync(0xffffffffu, e.x, j), lo2 = __shfl_sync(0xffffffffu, e.y, j);
-      const int c2 = __shfl_sync(0xffffffffu, e.w, j), ex0 = __shfl_sync(0xffffffffu, excl, j);
-      const int nr = __shfl_sync(0xffffffffu, nruns, j);
-      uint32_t nearmask = 0;  // steps of this lane's run left to FP64
-      int s1 = 0, s2 = 0;
-      if (g < items) {
-        const int off = g - ex0, u = off / nr, r = off - u * nr;
-        const int v0 = r * kRun, m = min(kRun, c2 - v0);
-        s1 = lo1 + u;
-        const int s1n = s1 + 1 == n1 ? 0 : s1 + 1;
-        double p0[3], p1[3], q0[3], q1[3];
-        load3(P1, s1, p0);
-        load3(P1, s1n, p1);
-        const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
-        const float ee = dot3(ex, ey, ez, ex, ey, ez);
-        s2 = lo2 + v0;
-        load3(Q2, s2, q0);
-        SegWalk w = walk_start(p0, q0, ex, ey, ez);
-        float acc = 0.f, turns = 0.f;
+      vb -= nv;
+      if (mine) {
+        double p[3], q[3];
+        load3(P1, e.x, p);
+        load3(Q2, e.y, q);
+        const double ox = 0.5 * p[0] + 0.5 * q[0], oy = 0.5 * p[1] + 0.5 * q[1], oz = 0.5 * p[2] + 0.5 * q[2];
+        org[0][lane] = ox;
+        org[1][lane] = oy;
+        org[2][lane] = oz;
+        float4 prev = make_float4((float)(q[0] - ox), (float)(q[1] - oy), (float)(q[2] - oz), 0.f);
+        for (int r = 1; r <= e.w; ++r) {
+          const int t = e.y + r;
+          load3(Q2, t >= n2 ? t - n2 : t, q);
+          const float4 cur = make_float4((float)(q[0] - ox), (float)(q[1] - oy), (float)(q[2] - oz), 0.f);
+          const float fx = cur.x - prev.x, fy = cur.y - prev.y, fz = cur.z - prev.z;
+          prev.w = dot3(fx, fy, fz, fx, fy, fz);
+          sq[vb + r - 1] = prev;
+          prev = cur;
+        }
+        sq[vb + e.w] = prev;
+      }
+      // Rows in order of their length: rank the entries by cnt2 (counting
+      // sort by ballots), then number the rows of the sorted entries.
+      const int key = mine ? e.w : 0;
+      int rank = 0, before = 0;
+      for (int k = 1; k <= 16; ++k) {
+        const unsigned m = __ballot_sync(0xffffffffu, key == k);
+        if (key == k) rank = before + __popc(m & lt);
+        before += __popc(m);
+      }
+      // Sorted position -> entry, and the row prefix in sorted order.
+      __shared__ int s_perm[kBkWarps][32];
+      if (mine) s_perm[wi][rank] = lane;
+      __syncwarp();
+      const int nact = before;  // active entries
+      const int pj = lane < nact ? s_perm[wi][lane] : 0;
+      const int rows_s = lane < nact ? __shfl_sync(0xffffffffu, e.z, pj) : 0;
+      int rpre = rows_s;
 #pragma unroll
-        for (int k = 0; k < kRun; ++k) {
-          if (k < m) {
-            const int t = s2 + k + 1;
-            load3(Q2, t == n2 ? 0 : t, q1);
-            if (!walk_step(w, p0, q1, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, rpre, o);
+        if (lane >= o) rpre += y;
+      }
+      const int nrows = __shfl_sync(0xffffffffu, rpre, 31);
+      rpre -= rows_s;  // exclusive
+      for (int base = 0; base < nrows; base += 32) {
+        const int g = base + lane;
+        // the last sorted entry whose rows start at or before row g
+        int i = 0;
+#pragma unroll
+        for (int st = 16; st; st >>= 1) {
+          const int x = __shfl_sync(0xffffffffu, rpre, i + st);
+          if (i + st < nact && x <= g) i += st;
+        }
+        const int j = __shfl_sync(0xffffffffu, pj, i);
+        const int u = g - __shfl_sync(0xffffffffu, rpre, i);
+        const int lo1 = __shfl_sync(0xffffffffu, e.x, j), lo2 = __shfl_sync(0xffffffffu, e.y, j);
+        const int c2 = __shfl_sync(0xffffffffu, e.w, j), vbj = __shfl_sync(0xffffffffu, vb, j);
+        const bool act = g < nrows;
+        // The warp walks as far as its longest row (rows are sorted).
+        const int wmax = __reduce_max_sync(0xffffffffu, act ? c2 : 0);
+        uint32_t nearmask = 0;  // steps of this lane's row left to FP64
+        int s1 = 0;
+        if (act) {
+          s1 = lo1 + u;
+          if (s1 >= n1) s1 -= (int)n1;
+          const int s1n = s1 + 1 == n1 ? 0 : s1 + 1;
+          double p0[3], p1[3];
+          load3(P1, s1, p0);
+          load3(P1, s1n, p1);
+          const double ox = org[0][j], oy = org[1][j], oz = org[2][j];
+          const float p0x = (float)(p0[0] - ox), p0y = (float)(p0[1] - oy), p0z = (float)(p0[2] - oz);
+          const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
+          const float ee = dot3(ex, ey, ez, ex, ey, ez);
+          float4 q0 = sq[vbj];
+          SegWalkF w = walk_start_f(p0x, p0y, p0z, q0, ex, ey, ez);
+          float acc = 0.f, turns = 0.f;
+          for (int k = 0; k < wmax; ++k) {
+            if (k < c2) {
+              const float4 q1 = sq[vbj + k + 1];
+              if (!walk_step_f(w, p0x, p0y, p0z, q1, q0.w, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
+              q0 = q1;
+            }
+          }
+          sum += kInvTwoPi * (double)acc + (double)turns;
+        }
+        // Queue this pass's FP64 pairs, one per lane per round; evaluate 32 at a time.
+        while (__any_sync(0xffffffffu, nearmask != 0)) {
+          const bool has = nearmask != 0;
+          const unsigned bm = __ballot_sync(0xffffffffu, has);
+          if (has) {
+            const int k = __ffs(nearmask) - 1;
+            nearmask &= nearmask - 1;
+            int s2 = lo2 + k;
+            if (s2 >= n2) s2 -= (int)n2;
+            nq[nn + __popc(bm & lt)] = make_int2(s1, s2);
+          }
+          nn += __popc(bm);
+          __syncwarp();
+          if (nn >= 32) {
+            const int2 q = nq[nn - 32 + lane];
+            sum += seg_term_fp64(A.xyz, o1 + q.x, o1 + (q.x + 1 == n1 ? 0 : q.x + 1), o2 + q.y,
+                                 o2 + (q.y + 1 == n2 ? 0 : q.y + 1));
+            nn -= 32;
+            __syncwarp();
           }
         }
-        sum += kInvTwoPi * (double)acc + (double)turns;
       }
-      // Queue this pass's FP64 pairs, one per lane per round; evaluate 32 at a time.
-      while (__any_sync(0xffffffffu, nearmask != 0)) {
-        const bool has = nearmask != 0;
-        const unsigned bm = __ballot_sync(0xffffffffu, has);
-        if (has) {
-          const int k = __ffs(nearmask) - 1;
-          nearmask &= nearmask - 1;
-          nq[nn + __popc(bm & ((1u << lane) - 1))] = make_int2(s1, s2 + k);
-        }
-        nn += __popc(bm);
-        __syncwarp();
-        if (nn >= 32) {
-          const int2 q = nq[nn - 32 + lane];
-          sum += seg_term_fp64(A.xyz, o1 + q.x, o1 + (q.x + 1 == n1 ? 0 : q.x + 1), o2 + q.y,
-                               o2 + (q.y + 1 == n2 ? 0 : q.y + 1));
-          nn -= 32;
-          __syncwarp();
-        }
-      }
+      __syncwarp();
     }
     if (lane < nn) {
       const int2 q = nq[lane];
@@ -1359,7 +1488,6 @@ __global__ void __launch_bounds__(256, FLN_BUCKET_MIN_CTAS) bh_buckets(BucketArg
                            o2 + (q.y + 1 == n2 ? 0 : q.y + 1));
     }
     __syncwarp();
-    nexact += pairs;
 #pragma unroll
     for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (lane == 0) fix_add(A.acc_lk + slot, sum);
@@ -2500,7 +2628,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       FLN_CUDA(cudaGetLastError());
       BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc_exact, d_counts};
       FLN_CUDA(cudaEventRecord(ctx.ev_bk[0], st));
-      bh_buckets<<<ctx.num_sms * 8, 256, 0, st>>>(BA);
+      bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, st>>>(BA);
       FLN_CUDA(cudaGetLastError());
       FLN_CUDA(cudaEventRecord(ctx.ev_bk[1], st));
       launches += 2;

@@ -77,7 +77,8 @@ int main(int argc, char **argv) {
     p.barnes_hut_init_beta = std::stod(f["barnes_hut_init_beta"]);
     p.barnes_hut_beta_limit = std::stod(f["barnes_hut_beta_limit"]);
     if (f["precision"] == "fp64") p.precision = FLN_PREC_FP64;
-    cert.ComputeFromModel(model, direct, disc, p.barnes_hut_init_beta, p.barnes_hut_beta_limit, engine);
+    else if (f["precision"] != "mixed") throw std::runtime_error("Invalid precision: '" + f["precision"] + "'.");
+    cert.ComputeFromModel(model, direct, disc, p, engine);
     const fln_stats s = engine.stats();
     std::cout << "Linking-Number Computation, Mean Off-Integer Error: " << s.mean_off_integer << std::endl;
     std::cout << "Linking-Number Computation, Max  Off-Integer Error: " << s.max_off_integer << std::endl;

@@ -87,8 +87,14 @@ class LinkingNumberCertificate {
     fln_default_params(&p);
     p.barnes_hut_init_beta = barnes_hut_init_beta;
     p.barnes_hut_beta_limit = barnes_hut_beta_limit;
+    ComputeFromModel(model, force_direct_sum, discretize, p, engine);
+  }
+  /* The same with every engine parameter (fln_params: precision, tree,
+   * schedule, ...). */
+  void ComputeFromModel(const Model &model, bool force_direct_sum, bool discretize, const fln_params &params,
+                        Engine &engine = Engine::Default()) {
     fln_certificate *c = nullptr;
-    fln_throw_if(fln_certificate_compute(engine.get(), model.get(), force_direct_sum, discretize, &p, &c));
+    fln_throw_if(fln_certificate_compute(engine.get(), model.get(), force_direct_sum, discretize, &params, &c));
     c_.reset(c);
   }
   void ExportToFile(const std::string &filename) const { fln_throw_if(fln_certificate_save(need(), filename.c_str())); }
