@@ -307,12 +307,16 @@ def run_ours(args, rank, world, local_rank):
         alg = BH_BYTES_PER_NODE_PAIR * far + BH_BYTES_PER_EXACT_ENTRY * ent
         achieved = alg / (trav_ms * 1e-3) / 1e9
         traffic = args.traffic_bytes_per_node_pair * node_pairs if args.traffic_bytes_per_node_pair else None
+        dram_gbs = traffic / (trav_ms * 1e-3) / 1e9 if traffic else None
         roof = {"bound": "hbm", "kernel": "bh_traverse", "achieved": achieved,
                 "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "frac_basis": "algorithmic bytes (2 x 184 B per far node pair, 2 x 32 B per exact entry)",
                 "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg, "far_node_pairs_per_step": far,
                 "exact_node_pairs_per_step": ent, "ms_per_launch": trav_ms,
-                "dram_gbs": traffic / (trav_ms * 1e-3) / 1e9 if traffic else None,
+                "dram_gbs": dram_gbs, "dram_frac": dram_gbs / peaks["hbm_gbs"] if dram_gbs else None,
+                "limiter": "L1 wavefronts and dependent-load latency (node records are re-read from L1/L2); "
+                           "DRAM runs at dram_frac of the copy peak",
                 "exact_kernel": {"kernel": "bh_buckets", "ms_per_step": exact_ms,
                                  "segment_pairs_per_step": seg_exact,
                                  "Gsegpair_per_s": seg_exact / (exact_ms * 1e-3) / 1e9 if exact_ms > 0 else None},
@@ -344,11 +348,26 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof,
         "clocks": clk,
         "stats": {"pairs": npairs, "segment_pairs": units, "beta_retried": s_last["beta_retried"],
+                  "retry_ms": s_last["ms_retry"], "front_records": s_last["bh_front_records"],
+                  "retry_from_roots": s_last["bh_retry_from_roots"], "rounds": s_last["bh_rounds"],
                   "escalated": s_last["bh_escalated"], "wait_timeouts": s_last["bh_wait_timeouts"],
                   "fp64_recomputed": s_last["fp64_recomputed"], "tree_build_ms": s_last["ms_tree_build"],
                   "far_evals": s_last["bh_far_evals"], "leaf_evals": s_last["bh_leaf_evals"],
                   "nonzero_links": int(np.sum(np.round(lk) != 0)), "flags_recomputed": int(np.sum(flags & 1))},
     }
+    fx = os.path.join(REPO, "tests", "golden", "configs", args.workload + ".npz")
+    if args.method == "barneshut" and os.path.exists(fx) and rank == 0:
+        # The FP64 direct-sum certificate of this workload (every pair), when
+        # one was made for it: the integers must agree byte for byte.
+        z = np.load(fx)
+        meta = json.loads(str(z["meta"]))
+        if meta["seed"] == args.seed and meta["pairs"] == npairs and (args.loops, args.loop_steps) == (200, 50000):
+            from fastlinkingnumbers_b200 import workloads as W
+            want = open(os.path.join(REPO, "tests", "golden", "configs", args.workload + ".txt")).read()
+            result["fp64_certificate"] = {
+                "certificate_equal": W.certificate_text(len(poff) - 1, pairs, lk) == want,
+                "max_abs_dev_vs_fp64": float(np.abs(lk - z["lk"]).max()),
+                "fp64_direct_kernel_s": meta.get("fp64_kernel_s")}
     if rank == 0 and world == 1 and args.direct_sample > 0:
         # Plain FP64 GPU direct sum and the mixed direct sum on a seeded sample
         # of pairs, extrapolated by segment pairs (the full FP64 direct sum of

@@ -411,39 +411,46 @@ void prepare(Model &m, bool discretize_on) {
     }
     for (auto &l : links) std::sort(l.begin(), l.end());
     discretize(m.curves, links, m.poly_offsets, m.poly_xyz, m.rounds);
-  } else {
-    m.poly_offsets.assign(nc + 1, 0);
+    // Potential pairs of the polylines (boxes of their segments).
+#pragma omp parallel for schedule(dynamic)
     for (int i = 0; i < nc; ++i) {
-      if (m.curves[i].kind != kPolyline && !m.curves[i].q.empty())
-        throw Error(FLN_ERR_INVALID_ARGUMENT, "Without Discretize the input model must be polylines.");
-      m.poly_offsets[i + 1] = m.poly_offsets[i] + (int64_t)m.curves[i].q.size();
+      Box3 b;
+      const int64_t a = m.poly_offsets[i], e = m.poly_offsets[i + 1], n = e - a;
+      for (int64_t k = 0; k < n; ++k) {
+        const double *p = &m.poly_xyz[3 * (a + k)], *q = &m.poly_xyz[3 * (a + (k + 1) % n)];
+        Box3 s;
+        for (int d = 0; d < 3; ++d) {
+          s.lo[d] = min_of(p[d], q[d]);
+          s.hi[d] = max_of(p[d], q[d]);
+        }
+        grow(b, s);
+      }
+      boxes[i] = b;
     }
+  } else {
+    // Without Discretize (lnc.cpp:371-379) the potential pairs come from the
+    // curves' own boxes, and the linking-number stage reads each looped curve
+    // as the closed polyline of its segment start points
+    // (Curve::GetStartPoints, curve.cpp:133-143: get_point(k, 0) for every
+    // segment k; a polyline's control points themselves). An open curve
+    // keeps its control points: it may not reach that stage.
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < nc; ++i) boxes[i] = m.curves[i].whole_box();
+    m.poly_offsets.assign(nc + 1, 0);
+    for (int i = 0; i < nc; ++i) m.poly_offsets[i + 1] = m.poly_offsets[i] + (int64_t)m.curves[i].q.size();
     m.poly_xyz.resize(3 * m.poly_offsets[nc]);
-    for (int i = 0; i < nc; ++i)
-      for (size_t k = 0; k < m.curves[i].q.size(); ++k) {
-        const Vec3 &v = m.curves[i].q[k];
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < nc; ++i) {
+      const CurveData &c = m.curves[i];
+      for (size_t k = 0; k < c.q.size(); ++k) {
+        const Vec3 v = (c.closed && c.kind != kPolyline) ? c.at((int)k, 0.0) : c.q[k];
         double *o = &m.poly_xyz[3 * (m.poly_offsets[i] + (int64_t)k)];
         o[0] = v.x;
         o[1] = v.y;
         o[2] = v.z;
       }
-    m.rounds = 0;
-  }
-  // Potential pairs of the polylines (boxes of their segments).
-#pragma omp parallel for schedule(dynamic)
-  for (int i = 0; i < nc; ++i) {
-    Box3 b;
-    const int64_t a = m.poly_offsets[i], e = m.poly_offsets[i + 1], n = e - a;
-    for (int64_t k = 0; k < n; ++k) {
-      const double *p = &m.poly_xyz[3 * (a + k)], *q = &m.poly_xyz[3 * (a + (k + 1) % n)];
-      Box3 s;
-      for (int d = 0; d < 3; ++d) {
-        s.lo[d] = min_of(p[d], q[d]);
-        s.hi[d] = max_of(p[d], q[d]);
-      }
-      grow(b, s);
     }
-    boxes[i] = b;
+    m.rounds = 0;
   }
   const auto pl = box_pairs(boxes);
   // An open curve that reaches the linking-number stage is an error there
