@@ -490,6 +490,91 @@ void exclusive_scan_i32(Context &ctx, DevBuf &tmp, const int32_t *in, int32_t *o
   FLN_CUDA(cub::DeviceScan::ExclusiveSum(t, bytes, in, out, (int)n, ctx.stream));
 }
 
+// Potential-link search on the device (potential_link_search.cpp:88-127):
+// every pair i < j of curves whose closed boxes meet (box[6c..6c+2] low
+// corner, [6c+3..6c+5] high corner; a box with lo.x > hi.x is empty and meets
+// nothing), in (i, j) order, as the host sweep (box_pairs) returns it. Tiled
+// all-pairs test: a CTA takes kJoinTile curves i and walks the tiles of j from
+// its own, staged in shared memory. The first pass counts each i's partners,
+// a scan turns the counts into offsets, the second pass writes each i's
+// partners in increasing j. Same comparisons as the host, so the same set.
+constexpr int kJoinTile = 256;
+
+template <bool kWrite>
+__global__ void __launch_bounds__(kJoinTile) box_join(const double *box, int nc, const int64_t *offs, int32_t *counts,
+                                                      int2 *out) {
+  __shared__ double s_b[6][kJoinTile];
+  const int i0 = blockIdx.x * kJoinTile, i = i0 + threadIdx.x;
+  double a[6];
+  bool va = false;
+  if (i < nc) {
+    for (int d = 0; d < 6; ++d) a[d] = box[6 * (int64_t)i + d];
+    va = a[0] <= a[3];
+  }
+  int64_t at = (kWrite && i < nc) ? offs[i] : 0;
+  int cnt = 0;
+  for (int j0 = i0; j0 < nc; j0 += kJoinTile) {
+    __syncthreads();
+    for (int x = threadIdx.x; x < 6 * kJoinTile; x += kJoinTile) {
+      const int jj = x / 6, d = x - 6 * jj;
+      s_b[d][jj] = j0 + jj < nc ? box[6 * (int64_t)(j0 + jj) + d] : 1.0;
+    }
+    __syncthreads();
+    if (!va) continue;
+    const int jn = min(kJoinTile, nc - j0);
+    for (int jj = 0; jj < jn; ++jj) {
+      const int j = j0 + jj;
+      if (j <= i) continue;
+      const double l0 = s_b[0][jj], l1 = s_b[1][jj], l2 = s_b[2][jj];
+      const double h0 = s_b[3][jj], h1 = s_b[4][jj], h2 = s_b[5][jj];
+      const bool hit = l0 <= h0 && a[0] <= h0 && a[1] <= h1 && a[2] <= h2 && l0 <= a[3] && l1 <= a[4] &&
+                       l2 <= a[5];
+      if (hit) {
+        if (kWrite) out[at++] = make_int2(i, j);
+        else ++cnt;
+      }
+    }
+  }
+  if (!kWrite && i < nc) counts[i] = cnt;
+}
+
+// The sorted pairs of the boxes in d_box (nc curves) on the host; curves
+// with empty[c] set get an empty box first. Beyond kJoinMaxCurves curves the
+// all-pairs test costs more than the host sweep, which then runs instead.
+constexpr int kJoinMaxCurves = 1 << 17;
+std::vector<Box3> boxes_to_host(Context &ctx, const double *d_box, int nc);
+std::vector<std::pair<int, int>> device_box_pairs(Context &ctx, const double *d_box, int nc) {
+  if (nc > kJoinMaxCurves) return box_pairs(boxes_to_host(ctx, d_box, nc));
+  std::vector<std::pair<int, int>> pl;
+  if (nc < 2) return pl;
+  cudaStream_t st = ctx.stream;
+  const int grid = (nc + kJoinTile - 1) / kJoinTile;
+  int32_t *d_cnt = static_cast<int32_t *>(ctx.d_disc[4].need((size_t)nc * sizeof(int32_t) + 16));
+  box_join<false><<<grid, kJoinTile, 0, st>>>(d_box, nc, nullptr, d_cnt, nullptr);
+  FLN_CUDA(cudaGetLastError());
+  std::vector<int32_t> cnt(nc);
+  FLN_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, nc * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaStreamSynchronize(st));
+  std::vector<int64_t> offs(nc);
+  int64_t total = 0;
+  for (int c = 0; c < nc; ++c) {
+    offs[c] = total;
+    total += cnt[c];
+  }
+  if (total == 0) return pl;
+  int64_t *d_offs = static_cast<int64_t *>(ctx.d_disc[5].need((size_t)nc * sizeof(int64_t) + (size_t)total * 8));
+  int2 *d_out = reinterpret_cast<int2 *>(d_offs + nc);
+  FLN_CUDA(cudaMemcpyAsync(d_offs, offs.data(), nc * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  box_join<true><<<grid, kJoinTile, 0, st>>>(d_box, nc, d_offs, nullptr, d_out);
+  FLN_CUDA(cudaGetLastError());
+  std::vector<int2> h((size_t)total);
+  FLN_CUDA(cudaMemcpyAsync(h.data(), d_out, total * sizeof(int2), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaStreamSynchronize(st));
+  pl.resize((size_t)total);
+  for (int64_t k = 0; k < total; ++k) pl[k] = {h[k].x, h[k].y};
+  return pl;
+}
+
 std::vector<Box3> boxes_to_host(Context &ctx, const double *d_box, int nc) {
   std::vector<double> h(6 * (size_t)nc);
   if (nc > 0)
@@ -650,7 +735,7 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
       double *d_box = buf<double>(B[27], 6 * (int64_t)nc);
       if (nc > 0) root_boxes<<<(nc + 127) / 128, 128, 0, st>>>(d_nodes, d_loff, nc, d_box);
       FLN_CUDA(cudaGetLastError());
-      const auto pl = box_pairs(boxes_to_host(ctx, d_box, nc));
+      const auto pl = device_box_pairs(ctx, d_box, nc);
       for (auto &p : pl) {
         slot_curves.push_back(p.first);
         slot_curves.push_back(p.second);
@@ -770,10 +855,8 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
   double *d_box = buf<double>(B[27], 6 * (int64_t)nc);
   if (nc > 0) polyline_boxes<<<nc, 256, 0, st>>>(d_xyz, d_out, d_box);
   FLN_CUDA(cudaGetLastError());
-  std::vector<Box3> pb = boxes_to_host(ctx, d_box, nc);
-  for (int c = 0; c < nc; ++c)
-    if (offsets[c + 1] == offsets[c]) pb[c] = Box3();
-  const auto pl = box_pairs(pb);
+  // (A curve without vertices gets the empty box from polyline_boxes.)
+  const auto pl = device_box_pairs(ctx, d_box, nc);
   pairs_out.resize(2 * pl.size());
   for (size_t k = 0; k < pl.size(); ++k) {
     pairs_out[2 * k] = pl[k].first;

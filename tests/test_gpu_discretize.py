@@ -47,6 +47,15 @@ def test_chain_mail(engine):
     _same(lambda: Model().SetCurves(3, counts, xyz), engine)
 
 
+def test_chain_mail_full_sheet(engine):
+    # 10,000 rings: the device join of the loop boxes runs over 40 tiles of
+    # 256 curves, with ring boxes that overlap their 8 neighbours.
+    off, xyz = workloads.chain_mail()
+    counts = -np.diff(off).astype(np.int32)
+    _, _, pairs, _ = _same(lambda: Model().SetCurves(3, counts, xyz), engine)
+    assert len(pairs) > 30_000
+
+
 def test_polymer(engine):
     off, xyz = workloads.polymer(seed=41, n_loops=40, n_steps=20_000, cube=300.0)
     counts = -np.diff(off).astype(np.int32)
