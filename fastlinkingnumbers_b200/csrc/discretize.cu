@@ -542,6 +542,7 @@ __global__ void __launch_bounds__(kJoinTile) box_join(const double *box, int nc,
 // with empty[c] set get an empty box first. Beyond kJoinMaxCurves curves the
 // all-pairs test costs more than the host sweep, which then runs instead.
 constexpr int kJoinMaxCurves = 1 << 17;
+constexpr int kJoinBufs = 34;  // d_disc[34], [35]: the join's own (0..33 belong to Discretize)
 std::vector<Box3> boxes_to_host(Context &ctx, const double *d_box, int nc);
 std::vector<std::pair<int, int>> device_box_pairs(Context &ctx, const double *d_box, int nc) {
   if (nc > kJoinMaxCurves) return box_pairs(boxes_to_host(ctx, d_box, nc));
@@ -549,7 +550,7 @@ std::vector<std::pair<int, int>> device_box_pairs(Context &ctx, const double *d_
   if (nc < 2) return pl;
   cudaStream_t st = ctx.stream;
   const int grid = (nc + kJoinTile - 1) / kJoinTile;
-  int32_t *d_cnt = static_cast<int32_t *>(ctx.d_disc[4].need((size_t)nc * sizeof(int32_t) + 16));
+  int32_t *d_cnt = static_cast<int32_t *>(ctx.d_disc[kJoinBufs].need((size_t)nc * sizeof(int32_t) + 16));
   box_join<false><<<grid, kJoinTile, 0, st>>>(d_box, nc, nullptr, d_cnt, nullptr);
   FLN_CUDA(cudaGetLastError());
   std::vector<int32_t> cnt(nc);
@@ -562,7 +563,7 @@ std::vector<std::pair<int, int>> device_box_pairs(Context &ctx, const double *d_
     total += cnt[c];
   }
   if (total == 0) return pl;
-  int64_t *d_offs = static_cast<int64_t *>(ctx.d_disc[5].need((size_t)nc * sizeof(int64_t) + (size_t)total * 8));
+  int64_t *d_offs = static_cast<int64_t *>(ctx.d_disc[kJoinBufs + 1].need((size_t)nc * sizeof(int64_t) + (size_t)total * 8));
   int2 *d_out = reinterpret_cast<int2 *>(d_offs + nc);
   FLN_CUDA(cudaMemcpyAsync(d_offs, offs.data(), nc * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   box_join<true><<<grid, kJoinTile, 0, st>>>(d_box, nc, d_offs, nullptr, d_out);
@@ -865,7 +866,7 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
   // The working buffers (tens of GB for 10^8 segments) are not kept for the
   // linking-number stage that follows.
   FLN_CUDA(cudaStreamSynchronize(st));
-  for (int k = 0; k < 34; ++k) B[k].release();
+  for (int k = 0; k < 36; ++k) B[k].release();
 }
 
 }  // namespace fln

@@ -111,7 +111,7 @@ struct Context {
   // Learned criterion in use on this context, and training buffers.
   DevBuf d_mlp, d_learn[8];
   // Device Discretize (discretize.cu).
-  DevBuf d_disc[34];
+  DevBuf d_disc[36];
   LearnedCfg learned{nullptr, 0.f, 0.f, 0};
   Recording recording;
 
