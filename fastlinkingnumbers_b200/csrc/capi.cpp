@@ -266,7 +266,8 @@ static void prepare_device(Context &ctx, Model &m, bool discretize_on) {
     prepare(m, false);
     return;
   }
-  discretize_device(ctx, m.curves, m.poly_offsets, m.poly_xyz, m.pairs, m.rounds);
+  discretize_device(ctx, m.curves, m.bcc_xyz.empty() ? nullptr : m.bcc_xyz.data(), m.poly_offsets, m.poly_xyz,
+                    m.pairs, m.rounds);
   // An open curve that reaches the linking-number stage is an error there
   // (Curve::GetStartPoints, curve.cpp:126-128); one without pairs is not.
   for (size_t p = 0; p < m.pairs.size(); ++p)
@@ -801,6 +802,8 @@ fln_status fln_model_set_curves(fln_model *m, fln_seg_type type, int32_t ncurves
       for (int64_t k = 0; k < n; ++k, ++at) cs[i].q[k] = {xyz[3 * at], xyz[3 * at + 1], xyz[3 * at + 2]};
     }
     m->m.curves.swap(cs);
+    m->m.bcc_xyz.clear();
+    m->m.bcc_xyz.shrink_to_fit();
     m->m.prepared = false;
     m->prepared_disc = -1;
   });

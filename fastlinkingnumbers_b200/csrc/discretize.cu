@@ -478,6 +478,12 @@ __global__ void root_boxes(const DNode *nodes, const int64_t *loff, int nc, doub
   }
 }
 
+// float32 control points (as a BCC file stores them) -> FP64, exactly.
+__global__ void widen_f32(const float *src, int64_t n, double *dst) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    dst[k] = (double)src[k];
+}
+
 template <class T>
 T *buf(DevBuf &b, int64_t n) {
   return b.as<T>((size_t)std::max<int64_t>(n, 1));
@@ -542,7 +548,7 @@ __global__ void __launch_bounds__(kJoinTile) box_join(const double *box, int nc,
 // with empty[c] set get an empty box first. Beyond kJoinMaxCurves curves the
 // all-pairs test costs more than the host sweep, which then runs instead.
 constexpr int kJoinMaxCurves = 1 << 17;
-constexpr int kJoinBufs = 34;  // d_disc[34], [35]: the join's own (0..33 belong to Discretize)
+constexpr int kJoinBufs = 34;  // d_disc[34], [35]: the join's own; [36] the float32 upload (0..33: Discretize)
 std::vector<Box3> boxes_to_host(Context &ctx, const double *d_box, int nc);
 std::vector<std::pair<int, int>> device_box_pairs(Context &ctx, const double *d_box, int nc) {
   if (nc > kJoinMaxCurves) return box_pairs(boxes_to_host(ctx, d_box, nc));
@@ -592,8 +598,9 @@ std::vector<Box3> boxes_to_host(Context &ctx, const double *d_box, int nc) {
 
 }  // namespace
 
-void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::vector<int64_t> &offsets,
-                       DoubleArray &xyz, std::vector<int32_t> &pairs_out, int32_t &rounds) {
+void discretize_device(Context &ctx, const std::vector<CurveData> &curves, const float *bcc_f32,
+                       std::vector<int64_t> &offsets, DoubleArray &xyz, std::vector<int32_t> &pairs_out,
+                       int32_t &rounds) {
   const int nc = (int)curves.size();
   cudaStream_t st = ctx.stream;
   DevBuf *B = ctx.d_disc;
@@ -605,12 +612,15 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
     seg_off[c + 1] = seg_off[c] + std::max(curves[c].segments(), 0);
     kind[c] = curves[c].kind;
   }
-  DoubleArray cp(3 * (size_t)std::max<int64_t>(cp_off[nc], 1));
+  // The packed FP64 control points, unless the float32 ones of the BCC file
+  // are uploaded and widened on the device.
+  DoubleArray cp(bcc_f32 ? 0 : 3 * (size_t)std::max<int64_t>(cp_off[nc], 1));
   const int64_t nseg = seg_off[nc];
   DoubleArray norms((size_t)std::max<int64_t>(nseg, 1));
 #pragma omp parallel for schedule(dynamic, 16)
   for (int c = 0; c < nc; ++c) {
-    if (!curves[c].q.empty()) std::memcpy(&cp[3 * cp_off[c]], &curves[c].q[0].x, curves[c].q.size() * sizeof(Vec3));
+    if (!bcc_f32 && !curves[c].q.empty())
+      std::memcpy(&cp[3 * cp_off[c]], &curves[c].q[0].x, curves[c].q.size() * sizeof(Vec3));
     for (int s = 0; s < curves[c].segments(); ++s) {
       const Vec3 &p = curves[c].q[s];
       norms[seg_off[c] + s] = std::sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
@@ -628,7 +638,15 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
   int64_t *d_cpoff = buf<int64_t>(B[1], nc + 1);
   int32_t *d_kind = buf<int32_t>(B[2], nc);
   int64_t *d_segoff = buf<int64_t>(B[3], nc + 1);
-  copy_h2d(ctx, d_cp, cp.data(), 3 * cp_off[nc] * sizeof(double));
+  if (bcc_f32) {
+    const int64_t nf = 3 * cp_off[nc];
+    float *d_f = buf<float>(B[kJoinBufs + 2], std::max<int64_t>(nf, 1));
+    copy_h2d(ctx, d_f, bcc_f32, nf * sizeof(float));
+    if (nf > 0) widen_f32<<<(int)std::min<int64_t>((nf + 255) / 256, 1 << 20), 256, 0, st>>>(d_f, nf, d_cp);
+    FLN_CUDA(cudaGetLastError());
+  } else {
+    copy_h2d(ctx, d_cp, cp.data(), 3 * cp_off[nc] * sizeof(double));
+  }
   FLN_CUDA(cudaMemcpyAsync(d_cpoff, cp_off.data(), (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_kind, kind.data(), std::max(nc, 1) * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_segoff, seg_off.data(), (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
@@ -866,7 +884,7 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::
   // The working buffers (tens of GB for 10^8 segments) are not kept for the
   // linking-number stage that follows.
   FLN_CUDA(cudaStreamSynchronize(st));
-  for (int k = 0; k < 36; ++k) B[k].release();
+  for (int k = 0; k < 37; ++k) B[k].release();
 }
 
 }  // namespace fln

@@ -111,7 +111,7 @@ struct Context {
   // Learned criterion in use on this context, and training buffers.
   DevBuf d_mlp, d_learn[8];
   // Device Discretize (discretize.cu).
-  DevBuf d_disc[36];
+  DevBuf d_disc[37];
   LearnedCfg learned{nullptr, 0.f, 0.f, 0};
   Recording recording;
 
@@ -183,8 +183,11 @@ double learned_gradients(Context &ctx, const float *params, const float *X, cons
 // and after it, on the GPU: the same closed polylines (CSR offsets, xyz) and
 // sorted unique pairs (i < j) as the host path, bit for bit; rounds = the
 // refinement rounds run. Throws Error on the reference's failure conditions.
-void discretize_device(Context &ctx, const std::vector<CurveData> &curves, std::vector<int64_t> &offsets,
-                       DoubleArray &xyz, std::vector<int32_t> &pairs, int32_t &rounds);
+// bcc_f32: the same control points as float32 (curves in order, 3 per
+// point), or nullptr; when given they are uploaded as such and widened on the
+// device (the same doubles, half the copy).
+void discretize_device(Context &ctx, const std::vector<CurveData> &curves, const float *bcc_f32,
+                       std::vector<int64_t> &offsets, DoubleArray &xyz, std::vector<int32_t> &pairs, int32_t &rounds);
 
 // Host<->device copies on ctx.stream that return when the data has arrived.
 // Pinned host memory is copied directly; pageable memory goes in 64 MB

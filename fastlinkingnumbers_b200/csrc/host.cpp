@@ -111,12 +111,18 @@ void load_bcc(const std::string &path, Model &m) {
   }
   // Allocate here, serially: an allocation failure inside the parallel
   // region could not leave it as an exception.
-  for (uint64_t i = 0; i < h.ncurves; ++i) curves[i].q.resize(npts[i]);
+  std::vector<int64_t> first(h.ncurves + 1, 0);  // first point of each curve
+  for (uint64_t i = 0; i < h.ncurves; ++i) {
+    curves[i].q.resize(npts[i]);
+    first[i + 1] = first[i] + npts[i];
+  }
+  FloatArray f32(3 * (size_t)first[h.ncurves]);
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t i = 0; i < (int64_t)h.ncurves; ++i) {
     CurveData &c = curves[i];
     const int64_t n = npts[i];
     const unsigned char *src = base + at[i];
+    if (n) std::memcpy(&f32[3 * first[i]], src, 12 * (size_t)n);
     for (int64_t k = 0; k < n; ++k) {
       float v[3];
       std::memcpy(v, src + 12 * k, 12);
@@ -124,6 +130,7 @@ void load_bcc(const std::string &path, Model &m) {
     }
   }
   m.curves.swap(curves);
+  m.bcc_xyz.swap(f32);
   m.prepared = false;
 }
 

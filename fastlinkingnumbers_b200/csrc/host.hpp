@@ -44,9 +44,15 @@ struct NoInitAlloc : std::allocator<T> {
   }
 };
 using DoubleArray = std::vector<double, NoInitAlloc<double>>;
+using FloatArray = std::vector<float, NoInitAlloc<float>>;
 
 struct Model {
   std::vector<CurveData> curves;
+  // The control points as a BCC file stores them (float32, x y z, curves in
+  // order), kept by load_bcc so that the GPU prepare can upload 12 bytes per
+  // point and widen them on the device (exact). Empty once the curves are
+  // replaced by other means.
+  FloatArray bcc_xyz;
   // Prepared (discretized) closed polylines, CSR over loops, and the sorted
   // unique potential pairs (i < j) of those polylines.
   std::vector<int64_t> poly_offsets;

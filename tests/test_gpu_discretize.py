@@ -98,3 +98,18 @@ def test_open_curve_in_pair_is_an_error(engine):
     with pytest.raises(FlnError) as e:
         Model().SetCurves(3, counts, xyz).Prepare(True, engine=engine)
     assert e.value.status == 9  # FLN_ERR_UNLOOPED
+
+
+def test_float32_upload_of_bcc_points(engine, tmp_path):
+    # A model loaded from a BCC file keeps its float32 points and the GPU
+    # prepare uploads those (12 bytes per point) and widens them on the
+    # device; the same curves given as doubles take the FP64 upload. Same
+    # output bit for bit.
+    off, xyz = workloads.polymer(seed=43, n_loops=30, n_steps=20_000, cube=260.0)
+    path = str(tmp_path / "p.bcc")
+    workloads.write_bcc(path, (off, xyz))
+    a = Model().ImportFromFile(path).Prepare(True, engine=engine)
+    b = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz).Prepare(True, engine=engine)
+    assert a[3] == b[3]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+    assert np.array_equal(a[1].view(np.uint64), b[1].view(np.uint64))
