@@ -42,14 +42,14 @@ EXPORTED = [
     "fln_certificate_equals", "fln_certificate_export_diffs",
     "fln_learned_default_options", "fln_learned_train", "fln_learned_create", "fln_learned_destroy",
     "fln_learned_get", "fln_ctx_set_learned", "fln_learned_collect", "fln_learned_predict",
-    "fln_learned_gradients", "fln_model_prepare_device", "fln_autotune",
+    "fln_learned_gradients", "fln_model_prepare_device", "fln_autotune", "fln_autotune_direct",
 ]
 
 
 class TuneResult(C.Structure):
     _fields_ = [
         ("best_ms", C.c_double), ("default_ms", C.c_double), ("trials", C.c_int32),
-        ("sample_pairs", C.c_int32), ("best_budget", C.c_int32), ("reserved0", C.c_int32),
+        ("sample_pairs", C.c_int32), ("best_budget", C.c_int32), ("best_direct_tile", C.c_int32),
         ("best_beta", C.c_double), ("reserved", C.c_double * 3),
     ]
 
@@ -68,7 +68,8 @@ class Params(C.Structure):
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
         ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("bh_budget", C.c_int32),
         ("bh_bucket", C.c_int32), ("bh_retry_from_roots", C.c_int32), ("bh_spill_cap", C.c_int32),
-        ("bh_wait_polls", C.c_int64), ("reserved_params", C.c_double * 4),
+        ("bh_wait_polls", C.c_int64), ("direct_tile", C.c_int32), ("reserved_i0", C.c_int32),
+        ("reserved_params", C.c_double * 4),
     ]
 
 
@@ -165,6 +166,7 @@ def load():
     L.fln_model_prepare.argtypes = [vp, C.c_int, P(i32)]
     L.fln_model_prepare_device.argtypes = [vp, vp, C.c_int, P(i32)]
     L.fln_autotune.argtypes = [vp, vp, vp, i32, vp, i64, P(Params), i32, i64, P(Params), P(TuneResult)]
+    L.fln_autotune_direct.argtypes = [vp, vp, vp, i32, vp, i64, P(Params), i64, P(Params), P(TuneResult)]
     L.fln_model_prepared_sizes.argtypes = [vp, P(i64), P(i64)]
     L.fln_model_get_prepared.argtypes = [vp, vp, vp, vp]
     L.fln_certificate_compute.argtypes = [vp, vp, C.c_int, C.c_int, P(Params), P(vp)]

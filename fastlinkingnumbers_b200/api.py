@@ -104,6 +104,20 @@ class Engine:
                                      C.byref(res)))
         return out, res.as_dict()
 
+    def autotune_direct(self, xyz, loop_offsets, pairs, sample_pairs: int = 0,
+                        params: Optional[N.Params] = None, **overrides):
+        """Fastest direct-sum tile shape on a seeded sample of the pairs:
+        (tuned Params, result dict)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        off = np.ascontiguousarray(loop_offsets, dtype=np.int64)
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        prm = params if params is not None else default_params(**overrides)
+        out = N.Params()
+        res = N.TuneResult()
+        N.check(self._L.fln_autotune_direct(self._h, _ptr(xyz), _ptr(off), len(off) - 1, _ptr(pairs), len(pairs),
+                                            C.byref(prm), int(sample_pairs), C.byref(out), C.byref(res)))
+        return out, res.as_dict()
+
     # ---- learned opening criterion (no counterpart in the reference)
     def set_learned(self, model: Optional["LearnedCriterion"]):
         """Uses `model` for the Barnes–Hut opening decisions of this engine (None: off)."""

@@ -150,7 +150,7 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   if (!d_err) d_err = ctx.d_err.as<double>(std::max<int64_t>(np, 1));  // Barnes–Hut needs one
   if (method == FLN_METHOD_DIRECTSUM) {
     launches += direct_sum_device(ctx, d_xyz, d_off, h_off, h_pairs, prm.precision, prm.near_factor, d_lk,
-                                  prm.precision == FLN_PREC_MIXED ? &near_terms : nullptr);
+                                  prm.precision == FLN_PREC_MIXED ? &near_terms : nullptr, prm.direct_tile);
     if (d_err) FLN_CUDA(cudaMemsetAsync(d_err, 0, np * sizeof(double), ctx.stream));
     if (d_flags) FLN_CUDA(cudaMemsetAsync(d_flags, 0, np * sizeof(int32_t), ctx.stream));
   } else {
@@ -235,6 +235,8 @@ static fln_params resolved(const fln_params *p) {
     throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_retry_from_roots is 0 or 1");
   if (r.bh_spill_cap < 0 || r.bh_spill_cap > 8192) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_spill_cap in [0, 8192]");
   if (r.bh_wait_polls < 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_wait_polls must not be negative");
+  if (r.direct_tile < 0 || r.direct_tile >= kDirectTileShapes)
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "direct_tile in [0, " + std::to_string(kDirectTileShapes - 1) + "]");
   return r;
 }
 
@@ -327,6 +329,24 @@ void compute_pairs_host(Context &ctx, const double *xyz, const int64_t *loop_off
   ctx.stats.kernel_launches = launches;
   ctx.stats.ms_total = now_ms() - t0;
 }
+// A seeded sample (12345) of `want` pairs (0 = 2048; all when fewer), in
+// their original order, for the autotuners.
+static std::vector<int32_t> sample_of(const std::vector<int32_t> &h_all, int64_t npairs, int64_t want) {
+  if (want <= 0) want = 2048;
+  std::vector<int64_t> idx(npairs);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::mt19937_64 rng(12345);
+  std::shuffle(idx.begin(), idx.end(), rng);
+  idx.resize(std::min(want, npairs));
+  std::sort(idx.begin(), idx.end());
+  std::vector<int32_t> out(2 * idx.size());
+  for (size_t k = 0; k < idx.size(); ++k) {
+    out[2 * k] = h_all[2 * idx[k]];
+    out[2 * k + 1] = h_all[2 * idx[k] + 1];
+  }
+  return out;
+}
+
 // Host loops and pairs -> the context's device buffers (checked).
 void upload_loops(Context &ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops, const int32_t *pairs,
                   int64_t npairs, std::vector<int64_t> &h_off, std::vector<int32_t> &h_pairs, double **d_xyz,
@@ -678,6 +698,58 @@ fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float 
   });
 }
 
+fln_status fln_autotune_direct(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                               const int32_t *pairs, int64_t npairs, const fln_params *params, int64_t sample_pairs,
+                               fln_params *out, fln_tune_result *result) {
+  return guarded([&] {
+    if (!ctx || !out || npairs <= 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL argument or no pairs");
+    const fln_params base = resolved(params);
+    Context &c = *ctx->c;
+    std::vector<int64_t> h_off;
+    std::vector<int32_t> h_all;
+    double *d_xyz;
+    int64_t *d_off;
+    upload_loops(c, xyz, loop_offsets, nloops, pairs, npairs, h_off, h_all, &d_xyz, &d_off);
+    const std::vector<int32_t> h_pairs = sample_of(h_all, npairs, sample_pairs);
+    const int64_t np = (int64_t)h_pairs.size() / 2;
+    double *d_lk = c.d_lk.as<double>(np), *d_err = c.d_err.as<double>(np);
+    int32_t *d_fl = c.d_flags.as<int32_t>(np);
+    auto time_of = [&](const fln_params &p) {
+      double best = 1e300;
+      for (int rep = 0; rep < 2; ++rep) {
+        FLN_CUDA(cudaEventRecord(c.ev0, c.stream));
+        run_pairs(c, d_xyz, d_off, h_off, h_pairs, FLN_METHOD_DIRECTSUM, p, d_lk, d_err, d_fl);
+        FLN_CUDA(cudaEventRecord(c.ev1, c.stream));
+        best = std::min(best, (double)c.elapsed(c.ev0, c.ev1));
+      }
+      return best;
+    };
+    time_of(base);  // warm-up
+    fln_tune_result r{};
+    r.sample_pairs = (int32_t)np;
+    r.default_ms = time_of(base);
+    fln_params best = base;
+    r.best_ms = r.default_ms;
+    r.trials = 1;
+    for (int t = 0; t < kDirectTileShapes; ++t) {
+      if (t == base.direct_tile) continue;
+      fln_params p = base;
+      p.direct_tile = t;
+      const double ms = time_of(p);
+      ++r.trials;
+      if (ms < r.best_ms) {
+        r.best_ms = ms;
+        best = p;
+      }
+    }
+    r.best_direct_tile = best.direct_tile;
+    r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
+    r.best_beta = best.barnes_hut_init_beta;
+    *out = best;
+    if (result) *result = r;
+  });
+}
+
 fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
                         const int32_t *pairs, int64_t npairs, const fln_params *params, int32_t tune_beta,
                         int64_t sample_pairs, fln_params *out, fln_tune_result *result) {
@@ -690,20 +762,8 @@ fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_off
     double *d_xyz;
     int64_t *d_off;
     upload_loops(c, xyz, loop_offsets, nloops, pairs, npairs, h_off, h_all, &d_xyz, &d_off);
-    // Seeded sample of the pairs.
-    const int64_t want = sample_pairs > 0 ? sample_pairs : 2048;
-    std::vector<int64_t> idx(npairs);
-    std::iota(idx.begin(), idx.end(), 0);
-    std::mt19937_64 rng(12345);
-    std::shuffle(idx.begin(), idx.end(), rng);
-    idx.resize(std::min(want, npairs));
-    std::sort(idx.begin(), idx.end());
-    std::vector<int32_t> h_pairs(2 * idx.size());
-    for (size_t k = 0; k < idx.size(); ++k) {
-      h_pairs[2 * k] = h_all[2 * idx[k]];
-      h_pairs[2 * k + 1] = h_all[2 * idx[k] + 1];
-    }
-    const int64_t np = (int64_t)idx.size();
+    const std::vector<int32_t> h_pairs = sample_of(h_all, npairs, sample_pairs);
+    const int64_t np = (int64_t)h_pairs.size() / 2;
     double *d_lk = c.d_lk.as<double>(np), *d_err = c.d_err.as<double>(np);
     int32_t *d_fl = c.d_flags.as<int32_t>(np);
     auto time_of = [&](const fln_params &p) {

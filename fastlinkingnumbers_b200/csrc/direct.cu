@@ -47,8 +47,8 @@
 namespace fln {
 namespace {
 
-constexpr int kBlockSegs = 128;  // threads per CTA = curve-1 segments per item
-constexpr int kTile = 256;       // curve-2 vertices per shared-memory tile
+constexpr int kBlockSegs = 128;  // default: threads per CTA = curve-1 segments per item
+constexpr int kTile = 256;       // default: curve-2 vertices per shared-memory tile
 constexpr double kInvTwoPi = 0.15915494309189533576888376337251436;
 
 struct DirectArgs {
@@ -77,7 +77,8 @@ __device__ __forceinline__ double3 load_v(const double *xyz, int64_t v) {
   return make_double3(__ldg(xyz + 3 * v), __ldg(xyz + 3 * v + 1), __ldg(xyz + 3 * v + 2));
 }
 
-// Sum over the CTA; the result is valid in thread 0.
+// Sum over the CTA of kB threads; the result is valid in thread 0.
+template <int kB>
 __device__ __forceinline__ double block_sum(double v, double *s_red) {
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -85,7 +86,7 @@ __device__ __forceinline__ double block_sum(double v, double *s_red) {
   __syncthreads();
   double r = 0;
   if (threadIdx.x == 0)
-    for (int w = 0; w < kBlockSegs / 32; ++w) r += s_red[w];
+    for (int w = 0; w < kB / 32; ++w) r += s_red[w];
   return r;
 }
 
@@ -119,9 +120,12 @@ __device__ __forceinline__ void renorm(double &x, double &y) {
 }
 
 // ------------------------------------------------------------------ FP64
-__global__ void __launch_bounds__(kBlockSegs) direct_fp64_kernel(DirectArgs A) {
-  __shared__ double sx[kTile + 1], sy[kTile + 1], sz[kTile + 1];
-  __shared__ double s_red[kBlockSegs / 32];
+// Tile shape: kB threads per CTA (= curve-1 segments per item), kT curve-2
+// vertices per shared-memory tile.
+template <int kB, int kT>
+__global__ void __launch_bounds__(kB) direct_fp64_kernel(DirectArgs A) {
+  __shared__ double sx[kT + 1], sy[kT + 1], sz[kT + 1];
+  __shared__ double s_red[kB / 32];
   __shared__ long long s_item;
   for (;;) {
     __syncthreads();
@@ -134,7 +138,7 @@ __global__ void __launch_bounds__(kBlockSegs) direct_fp64_kernel(DirectArgs A) {
     const int l1 = A.loops[2 * slot], l2 = A.loops[2 * slot + 1];
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1;
     const int64_t o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
-    const int64_t i = blk * kBlockSegs + threadIdx.x;
+    const int64_t i = blk * kB + threadIdx.x;
     const bool active = i < n1;
     double3 p0 = make_double3(0, 0, 0), p1 = p0;
     if (active) {
@@ -142,10 +146,10 @@ __global__ void __launch_bounds__(kBlockSegs) direct_fp64_kernel(DirectArgs A) {
       p1 = load_v(A.xyz, o1 + (i + 1 == n1 ? 0 : i + 1));
     }
     double xs = 1.0, ys = 0.0, S = -1.0, turns = 0.0;
-    for (int64_t k0 = 0; k0 < n2; k0 += kTile) {
-      const int kt = (int)(n2 - k0 < kTile ? n2 - k0 : kTile);
+    for (int64_t k0 = 0; k0 < n2; k0 += kT) {
+      const int kt = (int)(n2 - k0 < kT ? n2 - k0 : kT);
       __syncthreads();
-      for (int t = threadIdx.x; t <= kt; t += kBlockSegs) {
+      for (int t = threadIdx.x; t <= kt; t += kB) {
         const int64_t kk = k0 + t;
         const double3 v = load_v(A.xyz, o2 + (kk == n2 ? 0 : kk));
         sx[t] = v.x;
@@ -190,7 +194,7 @@ __global__ void __launch_bounds__(kBlockSegs) direct_fp64_kernel(DirectArgs A) {
       }
     }
     const double v = active ? atan2(ys, xs) * kInvTwoPi + turns : 0.0;
-    const double s = block_sum(v, s_red);
+    const double s = block_sum<kB>(v, s_red);
     if (threadIdx.x == 0) A.partial[item] = s;
   }
 }
@@ -209,6 +213,7 @@ __device__ __forceinline__ float atan_small(float t) {
 
 // Minimum and maximum over the CTA of 7 values each (a box and a length);
 // the result is in out[0..6] (min) and out[7..13] (max) for every thread.
+template <int kB>
 __device__ __forceinline__ void block_minmax7(float *lo, float *hi, float (*s_box)[14], float *out) {
   for (int o = 16; o; o >>= 1)
     for (int v = 0; v < 7; ++v) {
@@ -224,7 +229,7 @@ __device__ __forceinline__ void block_minmax7(float *lo, float *hi, float (*s_bo
   __syncthreads();
   for (int v = 0; v < 14; ++v) {
     float r = s_box[0][v];
-    for (int w = 1; w < kBlockSegs / 32; ++w) r = v < 7 ? fminf(r, s_box[w][v]) : fmaxf(r, s_box[w][v]);
+    for (int w = 1; w < kB / 32; ++w) r = v < 7 ? fminf(r, s_box[w][v]) : fmaxf(r, s_box[w][v]);
     out[v] = r;
   }
 }
@@ -235,10 +240,11 @@ __device__ __forceinline__ void block_minmax7(float *lo, float *hi, float (*s_bo
 #define FLN_MIXED_ACC 0
 #endif
 
-__global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) {
-  __shared__ float4 sq[kTile + 1];  // xyz relative to the tile origin; w = length of segment t
-  __shared__ double s_red[kBlockSegs / 32];
-  __shared__ float s_box[kBlockSegs / 32][14];
+template <int kB, int kT>
+__global__ void __launch_bounds__(kB) direct_mixed_kernel(DirectArgs A) {
+  __shared__ float4 sq[kT + 1];  // xyz relative to the tile origin; w = length of segment t
+  __shared__ double s_red[kB / 32];
+  __shared__ float s_box[kB / 32][14];
   __shared__ long long s_item;
   const float INF = __int_as_float(0x7f800000);
   for (;;) {
@@ -252,7 +258,7 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
     const int l1 = A.loops[2 * slot], l2 = A.loops[2 * slot + 1];
     const int64_t o1 = A.off[l1], n1 = A.off[l1 + 1] - o1;
     const int64_t o2 = A.off[l2], n2 = A.off[l2 + 1] - o2;
-    const int64_t i = blk * kBlockSegs + threadIdx.x;
+    const int64_t i = blk * kB + threadIdx.x;
     const bool active = i < n1;
     double3 p0 = make_double3(0, 0, 0), p1 = p0;
     if (active) {
@@ -264,11 +270,11 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
     double acc = 0.0, near_turns = 0.0;
     int turns = 0;
     unsigned near_count = 0;
-    for (int64_t k0 = 0; k0 < n2; k0 += kTile) {
-      const int kt = (int)(n2 - k0 < kTile ? n2 - k0 : kTile);
+    for (int64_t k0 = 0; k0 < n2; k0 += kT) {
+      const int kt = (int)(n2 - k0 < kT ? n2 - k0 : kT);
       const double3 O = load_v(A.xyz, o2 + k0);
       __syncthreads();
-      for (int t = threadIdx.x; t <= kt; t += kBlockSegs) {
+      for (int t = threadIdx.x; t <= kt; t += kB) {
         const int64_t kk = k0 + t;
         const double3 v = load_v(A.xyz, o2 + (kk == n2 ? 0 : kk));
         sq[t] = make_float4((float)(v.x - O.x), (float)(v.y - O.y), (float)(v.z - O.z), 0.f);
@@ -289,7 +295,7 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
         lo[2] = fminf(r0z, r1z); hi[2] = fmaxf(r0z, r1z);
         hi[3] = len1;
       }
-      for (int t = threadIdx.x; t < kt; t += kBlockSegs) {
+      for (int t = threadIdx.x; t < kt; t += kB) {
         const float4 a = sq[t], b = sq[t + 1];
         const float fx = b.x - a.x, fy = b.y - a.y, fz = b.z - a.z;
         const float len = sqrtf(fx * fx + fy * fy + fz * fz);
@@ -300,7 +306,7 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
         hi[3] = fmaxf(hi[3], len);
       }
       float bx[14];
-      block_minmax7(lo, hi, s_box, bx);
+      block_minmax7<kB>(lo, hi, s_box, bx);
       __syncthreads();
       // Box gap between the CTA's curve-1 segments and this tile: no segment
       // pair can be near-singular when it exceeds near_factor x (longest segment).
@@ -378,7 +384,7 @@ __global__ void __launch_bounds__(kBlockSegs) direct_mixed_kernel(DirectArgs A) 
 #endif
     }
     const double v = active ? acc * kInvTwoPi + (double)turns + near_turns : 0.0;
-    const double s = block_sum(v, s_red);
+    const double s = block_sum<kB>(v, s_red);
     if (threadIdx.x == 0) A.partial[item] = s;
     if (near_count) atomicAdd(A.counter + 1, (unsigned long long)near_count);
   }
@@ -395,11 +401,49 @@ __global__ void reduce_items_kernel(const double *partial, const int64_t *item_s
   lk_out[order[s]] = acc;
 }
 
+// The tile shapes the direct sum can run with (fln_params.direct_tile), the
+// default first: (curve-1 segments per item = threads per CTA, curve-2
+// vertices per shared-memory tile).
+struct TileShape {
+  int block, tile;
+};
+constexpr TileShape kShapes[kDirectTileShapes] = {{128, 256}, {128, 128}, {128, 512},
+                                                  {256, 256}, {256, 512}, {64, 256}};
+static_assert(kShapes[0].block == kBlockSegs && kShapes[0].tile == kTile, "the default shape comes first");
+
+template <int kB, int kT>
+void launch_direct_t(cudaStream_t st, int sms, int precision, const DirectArgs &A) {
+  int per_sm = 0;
+  if (precision == FLN_PREC_FP64) {
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel<kB, kT>, kB, 0));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.items, (int64_t)sms * std::max(per_sm, 1)));
+    direct_fp64_kernel<kB, kT><<<grid, kB, 0, st>>>(A);
+  } else {
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel<kB, kT>, kB, 0));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.items, (int64_t)sms * std::max(per_sm, 1)));
+    direct_mixed_kernel<kB, kT><<<grid, kB, 0, st>>>(A);
+  }
+}
+
+void launch_direct(int shape, cudaStream_t st, int sms, int precision, const DirectArgs &A) {
+  switch (shape) {
+    case 1: launch_direct_t<128, 128>(st, sms, precision, A); break;
+    case 2: launch_direct_t<128, 512>(st, sms, precision, A); break;
+    case 3: launch_direct_t<256, 256>(st, sms, precision, A); break;
+    case 4: launch_direct_t<256, 512>(st, sms, precision, A); break;
+    case 5: launch_direct_t<64, 256>(st, sms, precision, A); break;
+    default: launch_direct_t<kBlockSegs, kTile>(st, sms, precision, A); break;
+  }
+}
+
 }  // namespace
 
 int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
                       const std::vector<int32_t> &h_pairs, int precision, double near_factor, double *d_lk_out,
-                      double *near_terms_out) {
+                      double *near_terms_out, int tile_shape) {
+  if (tile_shape < 0 || tile_shape >= kDirectTileShapes)
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "direct_tile in [0, " + std::to_string(kDirectTileShapes - 1) + "]");
+  const int kB = kShapes[tile_shape].block;
   const int64_t np = (int64_t)h_pairs.size() / 2;
   if (np == 0) return 0;
   // Plan: orient each pair so its longer loop is curve 1, and order slots by
@@ -418,7 +462,7 @@ int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     if (nseg(b) > nseg(a)) std::swap(a, b);
     loops[2 * s] = a;
     loops[2 * s + 1] = b;
-    start[s + 1] = start[s] + (nseg(a) + kBlockSegs - 1) / kBlockSegs;
+    start[s + 1] = start[s] + (nseg(a) + kB - 1) / kB;
   }
   const int64_t items = start[np];
   int32_t *d_loops = ctx.d_loops.as<int32_t>(2 * np + np);
@@ -431,17 +475,8 @@ int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_start, start.data(), (np + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
   FLN_CUDA(cudaMemsetAsync(d_counter, 0, 2 * sizeof(unsigned long long), ctx.stream));
   DirectArgs A{d_xyz, d_off, d_loops, d_start, (int32_t)np, items, d_partial, d_counter, (float)near_factor};
-  int per_sm = 0;
   FLN_CUDA(cudaEventRecord(ctx.ev2, ctx.stream));
-  if (precision == FLN_PREC_FP64) {
-    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel, kBlockSegs, 0));
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)ctx.num_sms * std::max(per_sm, 1)));
-    direct_fp64_kernel<<<grid, kBlockSegs, 0, ctx.stream>>>(A);
-  } else {
-    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel, kBlockSegs, 0));
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)ctx.num_sms * std::max(per_sm, 1)));
-    direct_mixed_kernel<<<grid, kBlockSegs, 0, ctx.stream>>>(A);
-  }
+  launch_direct(tile_shape, ctx.stream, ctx.num_sms, precision, A);
   FLN_CUDA(cudaGetLastError());
   FLN_CUDA(cudaEventRecord(ctx.ev3, ctx.stream));
   reduce_items_kernel<<<(int)((np + 255) / 256), 256, 0, ctx.stream>>>(d_partial, d_start, d_order, (int32_t)np,
@@ -654,18 +689,19 @@ extern "C" fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, co
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // The default tile shape (the planning kernel cuts items of kBlockSegs).
   DirectArgs A{d_xyz, d_loop_offsets, reinterpret_cast<const int32_t *>(scratch + kNaLoops),
                reinterpret_cast<const int64_t *>(scratch + kNaStart), (int32_t)npairs, h.total_items,
                reinterpret_cast<double *>(scratch + kNaPartial), reinterpret_cast<unsigned long long *>(scratch),
                (float)kDefaultNearFactor};
   if (precision == FLN_PREC_FP64) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel, kBlockSegs, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel<kBlockSegs, kTile>, kBlockSegs, 0);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));
-    direct_fp64_kernel<<<grid, kBlockSegs, 0, s>>>(A);
+    direct_fp64_kernel<kBlockSegs, kTile><<<grid, kBlockSegs, 0, s>>>(A);
   } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel, kBlockSegs, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel<kBlockSegs, kTile>, kBlockSegs, 0);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));
-    direct_mixed_kernel<<<grid, kBlockSegs, 0, s>>>(A);
+    direct_mixed_kernel<kBlockSegs, kTile><<<grid, kBlockSegs, 0, s>>>(A);
   }
   reduce_items_kernel<<<(int)((npairs + 255) / 256), 256, 0, s>>>(
       reinterpret_cast<const double *>(scratch + kNaPartial), reinterpret_cast<const int64_t *>(scratch + kNaStart),

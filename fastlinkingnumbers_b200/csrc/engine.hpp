@@ -136,9 +136,11 @@ constexpr double kDefaultNearFactor = 4.0;
 // memory. d_xyz/d_off describe the loops; h_off is the host copy of the
 // offsets; h_pairs the host copy of the pairs. Writes lk (per caller pair) to
 // d_lk_out. Returns the number of kernel launches.
+// tile_shape: index into the direct sum's tile shapes (fln_params.direct_tile).
+constexpr int kDirectTileShapes = 6;
 int direct_sum_device(Context &ctx, const double *d_xyz, const int64_t *d_off, const std::vector<int64_t> &h_off,
                       const std::vector<int32_t> &h_pairs, int precision, double near_factor, double *d_lk_out,
-                      double *near_terms_out);
+                      double *near_terms_out, int tile_shape = 0);
 
 // Barnes–Hut over the same inputs; err per pair after ERROR_EST_SCALE and the
 // reference's beta retry; flags gets FLN_PAIR_BETA_RETRIED. Returns launches.

@@ -107,6 +107,11 @@ typedef struct fln_params {
                                    a waiting warp gives up, after which the stage reruns with budgeted
                                    rounds (fln_stats.bh_wait_timeouts); 0 = 2^21, a few seconds; smaller
                                    values exist to test that path */
+  int32_t direct_tile;          /* direct sum tile shape (curve-1 segments per item x curve-2 vertices per
+                                   shared-memory tile): 0 = 128 x 256 (default), 1 = 128 x 128,
+                                   2 = 128 x 512, 3 = 256 x 256, 4 = 256 x 512, 5 = 64 x 256; chosen by
+                                   fln_autotune_direct. Sums change only in their rounding. */
+  int32_t reserved_i0;          /* zero */
   double reserved_params[4];    /* zero */
 } fln_params;
 
@@ -311,7 +316,7 @@ typedef struct fln_tune_result {
   int32_t trials;     /* settings timed */
   int32_t sample_pairs;
   int32_t best_budget;
-  int32_t reserved0;
+  int32_t best_direct_tile;  /* fln_autotune_direct */
   double best_beta;
   double reserved[3];
 } fln_tune_result;
@@ -319,6 +324,15 @@ typedef struct fln_tune_result {
 fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
                         const int32_t *pairs, int64_t npairs, const fln_params *params, int32_t tune_beta,
                         int64_t sample_pairs, fln_params *out, fln_tune_result *result);
+
+/* Autotuner of the direct sum. No counterpart in the reference. Times the
+ * direct sum (params->precision, with its margin check) on a seeded sample
+ * of the pairs (sample_pairs, 0 = 2048) for each tile shape of
+ * fln_params.direct_tile (device time, best of two runs); *out gets *params
+ * with the fastest shape, result->best_direct_tile the shape. */
+fln_status fln_autotune_direct(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,
+                               const int32_t *pairs, int64_t npairs, const fln_params *params, int64_t sample_pairs,
+                               fln_params *out, fln_tune_result *result);
 
 /* One pair, host arrays (compute_link.h:62-64 and :86-87). */
 fln_status fln_direct_pair(fln_ctx *ctx, const double *xyz1, int64_t n1, const double *xyz2,

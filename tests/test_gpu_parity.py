@@ -315,3 +315,19 @@ def test_autotune_budget_keeps_results(engine):
     assert rb["trials"] == 13 and tb.barnes_hut_init_beta in (1.5, 2.0, 2.5, 3.0)
     lk2, _, _ = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tb)
     assert np.array_equal(np.rint(lk2), np.rint(lk0))
+
+
+@pytest.mark.parametrize("prec,tol", [(N.PREC_FP64, 1e-9), (N.PREC_MIXED, 1e-5)])
+def test_direct_tile_shapes_and_autotune(engine, prec, tol, golden_dir):
+    # Every tile shape of the direct sum gives the oracle's sums within the
+    # precision's tolerance; the autotuner times them all and picks one.
+    _, off, xyz, pairs = _prepared("knittubebroken", golden_dir)
+    ref = np.load(os.path.join(GOLDEN, "pairs", "knittubebroken.npz"))["lk_direct"]
+    for t in range(6):
+        lk, _, _ = engine.linking_numbers(xyz, off, pairs, "directsum", precision=prec, direct_tile=t)
+        np.testing.assert_allclose(lk, ref, rtol=0, atol=tol)
+    tuned, res = engine.autotune_direct(xyz, off, pairs, precision=prec, sample_pairs=64)
+    assert res["trials"] == 6 and 0 <= res["best_direct_tile"] < 6
+    assert tuned.direct_tile == res["best_direct_tile"] and res["best_ms"] <= res["default_ms"]
+    with pytest.raises(FlnError):
+        engine.linking_numbers(xyz, off, pairs, "directsum", precision=prec, direct_tile=6)
