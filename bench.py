@@ -225,7 +225,8 @@ def run_ours(args, rank, world, local_rank):
         # Round budget only: the same node pairs, so results change only in the
         # rounding of partial sums (beta stays the reference's 2). Tuned on a
         # seeded sample of the pairs, untimed.
-        prm, tune = eng.autotune(pxyz, poff, pairs, tune_beta=False, sample_pairs=2048, params=prm)
+        prm, tune = eng.autotune(pxyz, poff, pairs, tune_beta=False, sample_pairs=2048, params=prm,
+                                 tune_bucket=bool(args.autotune_bucket) and not args.bh_bucket)
     d_xyz = torch.from_numpy(pxyz).cuda()
     d_off = torch.from_numpy(poff).cuda()
     d_pairs = torch.from_numpy(pairs).cuda()
@@ -482,6 +483,8 @@ def main():
                     help="fixed Barnes-Hut round budget (skips the autotuner); 0 = tuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune the Barnes-Hut round budget on a sample of the pairs before timing")
+    ap.add_argument("--autotune-bucket", type=int, default=1,
+                    help="let the autotuner also choose the exact-bucket size (unless --bh-bucket is given)")
     ap.add_argument("--learned-leg", type=int, default=1,
                     help="also train the learned opening criterion on another seed and time one step with it")
     args = ap.parse_args()

@@ -50,7 +50,8 @@ class TuneResult(C.Structure):
     _fields_ = [
         ("best_ms", C.c_double), ("default_ms", C.c_double), ("trials", C.c_int32),
         ("sample_pairs", C.c_int32), ("best_budget", C.c_int32), ("best_direct_tile", C.c_int32),
-        ("best_beta", C.c_double), ("reserved", C.c_double * 3),
+        ("best_beta", C.c_double), ("best_bucket", C.c_int32), ("reserved1", C.c_int32),
+        ("reserved", C.c_double * 2),
     ]
 
     def as_dict(self):

@@ -90,9 +90,10 @@ class Engine:
         return out.value
 
     def autotune(self, xyz, loop_offsets, pairs, tune_beta: bool = False, sample_pairs: int = 0,
-                 params: Optional[N.Params] = None, **overrides):
+                 params: Optional[N.Params] = None, tune_bucket: bool = False, **overrides):
         """Fastest Barnes-Hut settings on a seeded sample of the pairs:
-        (tuned Params, result dict). Beta is tuned only if tune_beta."""
+        (tuned Params, result dict). The round budget always; beta only if
+        tune_beta, the exact-bucket size only if tune_bucket."""
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         off = np.ascontiguousarray(loop_offsets, dtype=np.int64)
         pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
@@ -100,7 +101,8 @@ class Engine:
         out = N.Params()
         res = N.TuneResult()
         N.check(self._L.fln_autotune(self._h, _ptr(xyz), _ptr(off), len(off) - 1, _ptr(pairs), len(pairs),
-                                     C.byref(prm), int(tune_beta), int(sample_pairs), C.byref(out),
+                                     C.byref(prm), int(bool(tune_beta)) | (2 if tune_bucket else 0),
+                                     int(sample_pairs), C.byref(out),
                                      C.byref(res)))
         return out, res.as_dict()
 

@@ -745,6 +745,7 @@ fln_status fln_autotune_direct(fln_ctx *ctx, const double *xyz, const int64_t *l
     r.best_direct_tile = best.direct_tile;
     r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
     r.best_beta = best.barnes_hut_init_beta;
+    r.best_bucket = best.bh_bucket > 0 ? best.bh_bucket : 8;
     *out = best;
     if (result) *result = r;
   });
@@ -783,14 +784,36 @@ fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_off
     fln_params best = base;
     r.best_ms = r.default_ms;
     r.trials = 1;
+    const bool t_beta = (tune_beta & 1) != 0, t_bucket = (tune_beta & 2) != 0 && base.bh_tree == 0;
     const double betas[] = {1.5, 2.0, 2.5, 3.0};
     const int budgets[] = {128, 256, 512};
-    for (double b : betas) {
-      if (!tune_beta && b != base.barnes_hut_init_beta) continue;
+    auto try_budgets = [&](fln_params p) {
       for (int bud : budgets) {
-        fln_params p = base;
-        if (tune_beta) p.barnes_hut_init_beta = b;
         p.bh_budget = bud;
+        const double ms = time_of(p);
+        ++r.trials;
+        if (ms < r.best_ms) {
+          r.best_ms = ms;
+          best = p;
+        }
+      }
+    };
+    for (double b : betas) {
+      if (!t_beta && b != base.barnes_hut_init_beta) continue;
+      fln_params p = base;
+      if (t_beta) p.barnes_hut_init_beta = b;
+      try_budgets(p);
+    }
+    if (!t_beta && base.barnes_hut_init_beta != 1.5 && base.barnes_hut_init_beta != 2.0 &&
+        base.barnes_hut_init_beta != 2.5 && base.barnes_hut_init_beta != 3.0)
+      try_budgets(base);  // the caller's own beta
+    if (t_bucket) {
+      // Exact buckets of other sizes around the best setting so far (the
+      // node pairs change: real sums move within the Barnes-Hut error).
+      const fln_params around = best;
+      for (int bk : {4, 6, 10, 12, 16}) {
+        fln_params p = around;
+        p.bh_bucket = bk;
         const double ms = time_of(p);
         ++r.trials;
         if (ms < r.best_ms) {
@@ -799,20 +822,9 @@ fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_off
         }
       }
     }
-    if (!tune_beta && base.barnes_hut_init_beta != 1.5 && base.barnes_hut_init_beta != 2.0 &&
-        base.barnes_hut_init_beta != 2.5 && base.barnes_hut_init_beta != 3.0)
-      for (int bud : budgets) {  // the caller's own beta
-        fln_params p = base;
-        p.bh_budget = bud;
-        const double ms = time_of(p);
-        ++r.trials;
-        if (ms < r.best_ms) {
-          r.best_ms = ms;
-          best = p;
-        }
-      }
     r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
     r.best_beta = best.barnes_hut_init_beta;
+    r.best_bucket = best.bh_bucket > 0 ? best.bh_bucket : 8;
     *out = best;
     if (result) *result = r;
   });

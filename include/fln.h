@@ -306,10 +306,13 @@ fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float 
  * Times the stage (tree build, traversal, retry, escalation, margin check)
  * on a seeded sample of the given pairs, `sample_pairs` of them (0 = 2048;
  * all pairs when there are fewer), for each traversal round budget
- * {128, 256, 512} and, when tune_beta != 0, each initial beta
- * {1.5, 2, 2.5, 3} (beta changes the real sums within the Barnes-Hut error,
- * never the certificate). *out gets *params with the fastest setting;
- * *result the sample times (device time, best of two runs each). */
+ * {128, 256, 512}; with bit 0 of tune_beta, also each initial beta
+ * {1.5, 2, 2.5, 3}; with bit 1 (curve-order trees), then the exact-bucket
+ * sizes {4, 6, 10, 12, 16} around the best setting. Beta and the bucket
+ * change the real sums within the Barnes-Hut error, never the certificate;
+ * the budget changes only their rounding. *out gets *params with the
+ * fastest setting; *result the sample times (device time, best of two runs
+ * each). */
 typedef struct fln_tune_result {
   double best_ms;     /* sample time of the chosen setting */
   double default_ms;  /* sample time of *params as given */
@@ -318,7 +321,9 @@ typedef struct fln_tune_result {
   int32_t best_budget;
   int32_t best_direct_tile;  /* fln_autotune_direct */
   double best_beta;
-  double reserved[3];
+  int32_t best_bucket;
+  int32_t reserved1;
+  double reserved[2];
 } fln_tune_result;
 
 fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_offsets, int32_t nloops,

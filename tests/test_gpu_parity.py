@@ -315,6 +315,11 @@ def test_autotune_budget_keeps_results(engine):
     assert rb["trials"] == 13 and tb.barnes_hut_init_beta in (1.5, 2.0, 2.5, 3.0)
     lk2, _, _ = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tb)
     assert np.array_equal(np.rint(lk2), np.rint(lk0))
+    # The exact-bucket size changes the node pairs, never the integers.
+    tk, rk = engine.autotune(pxyz, poff, pairs, tune_bucket=True, sample_pairs=64)
+    assert rk["trials"] == 9 and rk["best_bucket"] in (4, 6, 8, 10, 12, 16)
+    lk3, _, _ = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tk)
+    assert np.array_equal(np.rint(lk3), np.rint(lk0))
 
 
 @pytest.mark.parametrize("prec,tol", [(N.PREC_FP64, 1e-9), (N.PREC_MIXED, 1e-5)])
