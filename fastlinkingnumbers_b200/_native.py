@@ -42,7 +42,7 @@ EXPORTED = [
     "fln_certificate_equals", "fln_certificate_export_diffs",
     "fln_learned_default_options", "fln_learned_train", "fln_learned_create", "fln_learned_destroy",
     "fln_learned_get", "fln_ctx_set_learned", "fln_learned_collect", "fln_learned_predict",
-    "fln_learned_gradients", "fln_model_prepare_device", "fln_autotune", "fln_autotune_direct",
+    "fln_learned_gradients", "fln_model_prepare_device", "fln_autotune", "fln_autotune_direct", "fln_learned_configure",
 ]
 
 
@@ -98,7 +98,7 @@ class LearnedOptions(C.Structure):
         ("s_min", C.c_double), ("sample_keep", C.c_double), ("max_samples", C.c_int64),
         ("max_terms", C.c_int64), ("epochs", C.c_int32), ("batch", C.c_int32),
         ("learning_rate", C.c_double), ("quantile", C.c_double), ("tau_quantile", C.c_double),
-        ("val_fraction", C.c_double), ("min_candidates", C.c_int32), ("reserved0", C.c_int32),
+        ("val_fraction", C.c_double), ("min_candidates", C.c_int32), ("min_node_segments", C.c_int32),
         ("seed", C.c_uint64), ("reserved", C.c_double * 4),
     ]
 
@@ -109,11 +109,12 @@ class LearnedInfo(C.Structure):
         ("val_samples", C.c_int64), ("s_min", C.c_double), ("log10_tau", C.c_double),
         ("min_candidates", C.c_int32), ("epochs", C.c_int32), ("train_loss", C.c_double),
         ("val_loss", C.c_double), ("val_coverage", C.c_double), ("ms_collect", C.c_double),
-        ("ms_train", C.c_double), ("reserved", C.c_double * 4),
+        ("ms_train", C.c_double), ("min_node_segments", C.c_int32), ("reserved_i", C.c_int32),
+        ("reserved", C.c_double * 3),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
 class FlnError(RuntimeError):
@@ -192,6 +193,7 @@ def load():
     L.fln_learned_train.argtypes = [vp, vp, vp, i32, vp, i64, P(Params), P(LearnedOptions), P(vp)]
     L.fln_learned_create.argtypes = [vp, f64, f64, i32, P(vp)]
     L.fln_learned_destroy.argtypes = [vp]
+    L.fln_learned_configure.argtypes = [vp, i32, i32]
     L.fln_learned_destroy.restype = None
     L.fln_learned_get.argtypes = [vp, vp, P(LearnedInfo)]
     L.fln_ctx_set_learned.argtypes = [vp, vp]

@@ -224,6 +224,13 @@ class LearnedCriterion:
         N.check(self._L.fln_learned_get(self._h, _ptr(p), None))
         return p
 
+    def configure(self, min_candidates: int = 4, min_node_segments: int = 0) -> "LearnedCriterion":
+        """When the MLP runs in the traversal: warp steps with at least
+        min_candidates candidates, candidates whose smaller node holds at
+        least min_node_segments segments. Applies at the next set_learned."""
+        N.check(self._L.fln_learned_configure(self._h, int(min_candidates), int(min_node_segments)))
+        return self
+
     def info(self) -> dict:
         i = N.LearnedInfo()
         N.check(self._L.fln_learned_get(self._h, None, C.byref(i)))

@@ -1065,6 +1065,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       double dsq = 0.0;
       float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
       float2 fr = make_float2(0.f, 0.f);
+      int mincnt = 0;  // segments of the smaller node (learned criterion)
       if (act) {
         const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
@@ -1074,6 +1075,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         fv = make_float4((float)dx, (float)dy, (float)dz, (float)dsq);
         fr = make_float2((float)h1.r, (float)h2.r);
         sep = (float)(sqrt(dsq) / rs);
+        if constexpr (kLearn) mincnt = min(h1.cnt, h2.cnt);
         if (leaf1 && leaf2) {
           kind = 1;
           ex = make_int4(h1.lo, h2.lo, 1, 1);
@@ -1111,7 +1113,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       // far-field pair. The warp's candidates are evaluated at once, and only
       // when there are at least min_cand (>= 1) of them.
       if constexpr (kLearn) {
-        const bool cand = kind == 3 && sep >= A.learned.s_min;
+        const bool cand = kind == 3 && sep >= A.learned.s_min && mincnt >= A.learned.min_seg;
         if (__popc(__ballot_sync(0xffffffffu, cand)) >= A.learned.min_cand) {
           float f[kMlpIn];
           for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
@@ -1501,9 +1503,17 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { travers
 // The first pass, which records its frontier for the beta retry.
 __global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_front(TravArgs A) { traverse<false, false, true>(A); }
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, false>(A); }
-// Three CTAs per SM (168 registers).
-__global__ void __launch_bounds__(32 * kWarps, 3) bh_traverse_learned(TravArgs A) { traverse<true, false, false>(A); }
-__global__ void __launch_bounds__(32 * kWarps, 3) bh_traverse_learned_front(TravArgs A) {
+// The learned kernels at FLN_LEARNED_MIN_CTAS CTAs per SM: their MLP code
+// (BF16 warp MMA) takes 168 registers at three CTAs; held to five, the
+// traversal keeps the plain kernel's occupancy and the inference, which runs
+// only for some warp steps, spills.
+#ifndef FLN_LEARNED_MIN_CTAS
+#define FLN_LEARNED_MIN_CTAS 5
+#endif
+__global__ void __launch_bounds__(32 * kWarps, FLN_LEARNED_MIN_CTAS) bh_traverse_learned(TravArgs A) {
+  traverse<true, false, false>(A);
+}
+__global__ void __launch_bounds__(32 * kWarps, FLN_LEARNED_MIN_CTAS) bh_traverse_learned_front(TravArgs A) {
   traverse<true, false, true>(A);
 }
 
@@ -2890,7 +2900,7 @@ void learned_collect(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   // with a proportionally lower keep rate, which keeps the sample uniform.
   for (int attempt = 0; attempt < 4; ++attempt) {
     FLN_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
-    ctx.learned = LearnedCfg{nullptr, 0.f, 0.f, 0};
+    ctx.learned = LearnedCfg{nullptr, 0.f, 0.f, 0, 0};
     ctx.recording.rec = d_rec;
     ctx.recording.count = d_cnt;
     ctx.recording.cap = cap;

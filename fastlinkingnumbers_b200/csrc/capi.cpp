@@ -630,6 +630,7 @@ fln_status fln_learned_train(fln_ctx *ctx, const double *xyz, const int64_t *loo
     inf.s_min = o.s_min;
     inf.log10_tau = log10_tau;
     inf.min_candidates = std::max(1, o.min_candidates);
+    inf.min_node_segments = std::max(0, o.min_node_segments);
     inf.epochs = o.epochs;
     inf.train_loss = train_loss;
     inf.val_loss = val_loss;
@@ -658,6 +659,16 @@ fln_status fln_learned_create(const float *params, double s_min, double log10_ta
 
 void fln_learned_destroy(fln_learned *m) { delete m; }
 
+fln_status fln_learned_configure(fln_learned *m, int32_t min_candidates, int32_t min_node_segments) {
+  return guarded([&] {
+    if (!m) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL model");
+    if (min_candidates < 1 || min_candidates > 32 || min_node_segments < 0)
+      throw Error(FLN_ERR_INVALID_ARGUMENT, "min_candidates in [1, 32], min_node_segments >= 0");
+    m->info.min_candidates = min_candidates;
+    m->info.min_node_segments = min_node_segments;
+  });
+}
+
 fln_status fln_learned_get(const fln_learned *m, float *params_out, fln_learned_info *info_out) {
   return guarded([&] {
     if (!m) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL model");
@@ -670,10 +681,10 @@ fln_status fln_ctx_set_learned(fln_ctx *ctx, const fln_learned *m) {
   return guarded([&] {
     if (!ctx) throw Error(FLN_ERR_INVALID_ARGUMENT, "NULL context");
     FLN_CUDA(cudaSetDevice(ctx->c->device));
-    if (!m) learned_enable(*ctx->c, nullptr, 0.f, 0.f, 0);
+    if (!m) learned_enable(*ctx->c, nullptr, 0.f, 0.f, 0, 0);
     else
       learned_enable(*ctx->c, m->params.data(), (float)m->info.s_min, (float)m->info.log10_tau,
-                     m->info.min_candidates);
+                     m->info.min_candidates, m->info.min_node_segments);
   });
 }
 

@@ -82,6 +82,7 @@ struct LearnedCfg {
   float s_min;          // candidates: separation |dr| / (r1 + r2) at least this
   float log10_tau;      // accept when the predicted log10 error is below this (at beta0)
   int32_t min_cand;     // run the MLP only when a warp step has at least this many candidates
+  int32_t min_seg;      // candidates: the smaller node holds at least this many segments
 };
 
 // Sampling of node pairs for training, during the first Barnes–Hut pass
@@ -201,6 +202,7 @@ void copy_d2h(Context &ctx, void *h_dst, const void *d_src, size_t bytes);
 void parallel_memcpy(void *dst, const void *src, size_t bytes);
 
 // Packs params into the context's device weights and enables the criterion.
-void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand);
+void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand,
+                    int32_t min_seg);
 
 }  // namespace fln

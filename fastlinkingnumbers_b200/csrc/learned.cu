@@ -303,16 +303,17 @@ double learned_gradients(Context &ctx, const float *params, const float *X, cons
   return loss;
 }
 
-void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand) {
+void learned_enable(Context &ctx, const float *params, float s_min, float log10_tau, int32_t min_cand,
+                    int32_t min_seg) {
   if (!params) {
-    ctx.learned = LearnedCfg{nullptr, 0.f, 0.f, 0};
+    ctx.learned = LearnedCfg{nullptr, 0.f, 0.f, 0, 0};
     return;
   }
   float *d_p = ctx.d_learn[7].as<float>(4 * kMlpParams + 4);
   FLN_CUDA(cudaMemcpyAsync(d_p, params, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, ctx.stream));
   MlpFrag *F = pack_device(ctx, d_p);
   FLN_CUDA(cudaStreamSynchronize(ctx.stream));
-  ctx.learned = LearnedCfg{F, s_min, log10_tau, std::max<int32_t>(1, min_cand)};
+  ctx.learned = LearnedCfg{F, s_min, log10_tau, std::max<int32_t>(1, min_cand), std::max<int32_t>(0, min_seg)};
 }
 
 }  // namespace fln

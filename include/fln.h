@@ -252,7 +252,8 @@ typedef struct fln_learned_options {
   double tau_quantile;    /* 0.5 */
   double val_fraction;    /* held-out share of the samples: 0.1 */
   int32_t min_candidates; /* the MLP runs for a warp step with at least this many candidates: 4 */
-  int32_t reserved0;
+  int32_t min_node_segments; /* only node pairs whose smaller node holds at least this many segments are
+                                candidates (where accepting a pair saves a subtree); 0 = every node */
   uint64_t seed;          /* 1 */
   double reserved[4];
 } fln_learned_options;
@@ -266,7 +267,9 @@ typedef struct fln_learned_info {
   double train_loss, val_loss; /* pinball loss */
   double val_coverage;    /* share of held-out samples whose true log10 error is <= the prediction */
   double ms_collect, ms_train;
-  double reserved[4];
+  int32_t min_node_segments;
+  int32_t reserved_i;
+  double reserved[3];
 } fln_learned_info;
 
 typedef struct fln_learned fln_learned;
@@ -279,6 +282,10 @@ fln_status fln_learned_train(fln_ctx *ctx, const double *xyz, const int64_t *loo
 fln_status fln_learned_create(const float *params, double s_min, double log10_tau, int32_t min_candidates,
                               fln_learned **out);
 void fln_learned_destroy(fln_learned *m);
+/* Changes when the model runs in the traversal (see fln_learned_options:
+ * min_candidates >= 1, min_node_segments >= 0); takes effect at the next
+ * fln_ctx_set_learned. */
+fln_status fln_learned_configure(fln_learned *m, int32_t min_candidates, int32_t min_node_segments);
 /* Either output may be NULL. */
 fln_status fln_learned_get(const fln_learned *m, float *params_out, fln_learned_info *info_out);
 /* NULL turns the criterion off. The context keeps its own device copy. */

@@ -127,3 +127,40 @@ def test_learned_criterion_rejects_other_schedules(engine, polymer_small):
             engine.linking_numbers(xyz, off, pairs[:10], "barneshut", bh_schedule=1)
     finally:
         engine.set_learned(None)
+
+
+def test_learned_time_on_default_path(engine):
+    # The default traversal (exact buckets of 8 segments, frontier retry):
+    # plain against learned, the MLP applied to every candidate and only to
+    # node pairs whose smaller node holds >= 32 segments. Device time of the
+    # whole stage, best of three runs each. Integers must agree; the measured
+    # times and node pairs are printed (and bounded: the learned run may not
+    # evaluate more node pairs than the plain one).
+    off_tr, xyz_tr, pairs_tr = _polymer(53, loops=60, steps=50_000, cube=250.0)
+    off, xyz, pairs = _polymer(54, loops=60, steps=50_000, cube=250.0)
+    model = LearnedCriterion.train(engine, xyz_tr, off_tr, pairs_tr)
+
+    def best_of(n=3):
+        runs = []
+        for _ in range(n):
+            lk, _, _ = engine.linking_numbers(xyz, off, pairs, "barneshut")
+            runs.append((engine.stats(), lk))
+        return min(runs, key=lambda r: r[0]["ms_kernels"])
+
+    s_p, lk_p = best_of()
+    res = {}
+    for min_seg in (0, 32):
+        model.configure(min_candidates=4, min_node_segments=min_seg)
+        engine.set_learned(model)
+        try:
+            res[min_seg] = best_of()
+        finally:
+            engine.set_learned(None)
+    work_p = s_p["bh_far_evals"] + s_p["bh_exact_entries"]
+    for min_seg, (s, lk) in res.items():
+        assert np.array_equal(np.rint(lk), np.rint(lk_p))
+        work = s["bh_far_evals"] + s["bh_exact_entries"]
+        print(f"learned (min_node_segments {min_seg}): {s['ms_kernels']:.2f} ms vs plain {s_p['ms_kernels']:.2f} ms "
+              f"({s['ms_kernels'] / s_p['ms_kernels']:.3f}x), node pairs {work:.5g} vs {work_p:.5g} "
+              f"({work / work_p:.4f}x)")
+        assert work <= work_p * 1.001
