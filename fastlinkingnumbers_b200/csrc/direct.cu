@@ -234,10 +234,12 @@ __device__ __forceinline__ void block_minmax7(float *lo, float *hi, float (*s_bo
   }
 }
 
-// Accumulation of a thread's terms over a tile: 0 = FP32, 1 = FP32 with
-// Kahan compensation, 2 = FP64.
+// Accumulation of a thread's terms over a tile: 0 = FP32 over the tile
+// (up to kT terms), 1 = FP32 with Kahan compensation, 2 = FP64 per term,
+// 3 = FP32 runs of 32 terms folded into FP64 (the rounding error of a run is
+// bounded by 32 terms instead of kT, for one FP64 add per 32 terms).
 #ifndef FLN_MIXED_ACC
-#define FLN_MIXED_ACC 0
+#define FLN_MIXED_ACC 3
 #endif
 
 template <int kB, int kT>
@@ -370,6 +372,12 @@ __global__ void __launch_bounds__(kB) direct_mixed_kernel(DirectArgs A) {
           accf += term;
 #endif
         }
+#if FLN_MIXED_ACC == 3
+        if ((k & 31) == 31) {
+          acc += (double)accf;
+          accf = 0.f;
+        }
+#endif
         q = qn;
         ax = dx; ay = dy; az = dz;
         bx_ = cx; by = cy; bz = cz;
