@@ -306,6 +306,8 @@ def run_ours(args, rank, world, local_rank):
         seg_exact = float(np.mean([s["bh_leaf_evals"] for s in st]))
         node_pairs = far + ent
         alg = BH_BYTES_PER_NODE_PAIR * far + BH_BYTES_PER_EXACT_ENTRY * ent
+        sm_ghz = (clk.get("sm_mhz") or 1965.0) / 1e3
+        fp32_bound = 148 * 128 * sm_ghz / 45.0  # G segment pairs / s
         achieved = alg / (trav_ms * 1e-3) / 1e9
         traffic = args.traffic_bytes_per_node_pair * node_pairs if args.traffic_bytes_per_node_pair else None
         dram_gbs = traffic / (trav_ms * 1e-3) / 1e9 if traffic else None
@@ -320,7 +322,12 @@ def run_ours(args, rank, world, local_rank):
                            "DRAM runs at dram_frac of the copy peak",
                 "exact_kernel": {"kernel": "bh_buckets", "ms_per_step": exact_ms,
                                  "segment_pairs_per_step": seg_exact,
-                                 "Gsegpair_per_s": seg_exact / (exact_ms * 1e-3) / 1e9 if exact_ms > 0 else None},
+                                 "Gsegpair_per_s": seg_exact / (exact_ms * 1e-3) / 1e9 if exact_ms > 0 else None,
+                                 "bound": "fp32 issue",
+                                 "bound_Gsegpair_per_s": fp32_bound,
+                                 "frac": (seg_exact / (exact_ms * 1e-3) / 1e9) / fp32_bound if exact_ms > 0 else None,
+                                 "bound_note": "45 FP32 FMA-pipe ops + 2 MUFU per segment pair (the algorithmic "
+                                               "count): 148 SMs x 128 lanes x SM clock / 45"},
                 "note": ("per step (all traversal rounds, CUDA events around each launch): algorithmic "
                          "bytes = 2 x 184 B FP32 node record per far-field node pair + 2 x 32 B (centre, "
                          "radius) per node pair handed to the exact list; traffic = DRAM read+write per "
