@@ -1410,7 +1410,10 @@ __global__ void __launch_bounds__(32 * kBkWarps, FLN_BUCKET_MIN_CTAS) bh_buckets
       __syncwarp();
       const int nact = before;  // active entries
       const int pj = lane < nact ? s_perm[wi][lane] : 0;
-      const int rows_s = lane < nact ? __shfl_sync(0xffffffffu, e.z, pj) : 0;
+      // (Every lane takes part in the shuffle; the rows of lanes past nact
+      // are dropped after it.)
+      const int rows_pj = __shfl_sync(0xffffffffu, e.z, pj);
+      const int rows_s = lane < nact ? rows_pj : 0;
       int rpre = rows_s;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
