@@ -2616,6 +2616,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         cur = 1 - cur;
         continue;
       }
+      if (!d_bkt) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut rounds without an exact list");
       TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
                  d_batch[1 - cur], cap, d_ctr + 1, budget, bucket, d_bkt, d_ctr + 2, bkt_soft, bkt_cap, d_acc,
                  d_acc_err, d_counts, d_spill, d_ctr, d_status,
@@ -2732,8 +2733,10 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       ctx.stats.bh_escalated = (int64_t)cnt[3];
       return launches;
     }
-    // A bounded wait ran out: redo the stage with budgeted rounds.
+    // A bounded wait ran out: redo the stage with budgeted rounds, which
+    // need the exact list the persistent schedule does not use.
     ctx.stats.bh_wait_timeouts += 1;
+    d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)bkt_cap * sizeof(BucketChunk)));
     d_status = reinterpret_cast<int32_t *>(d_counts + 2);
     FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
     FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
