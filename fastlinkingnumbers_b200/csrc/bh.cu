@@ -945,15 +945,27 @@ __device__ __forceinline__ void front_put(const TravArgs &A, long long &fr, int 
 // is written out as new batches for the next round, so a heavy loop pair
 // spreads over many warps while light pairs finish in one go.
 // kLearn: the learned opening criterion (A.learned); kRecord: sampling of
-// training node pairs (A.rec); kFront: frontier recording (A.front). The
-// plain instantiation has none of them.
+// training node pairs (A.rec). kMode: 0 plain; 1 the first pass, which
+// records its frontier (A.front); 2 the beta retry continued from a frontier
+// (A.in1 records).
 // Input: the batches in[0, nin), then the frontier records in1[0, nin1)
 // (up to kFrontPairs node pairs each), taken one at a time from A.queue.
-template <bool kLearn, bool kRecord, bool kFront>
+//
+// The continued retry (kMode 2) keeps the first pass's far-field and error
+// sums of the slot. A node pair's far-field value and estimate do not depend
+// on beta, so a frontier pair (marked by bit 31 of its first node id) that is
+// still far at the slot's beta is left alone: its value is already in the
+// sums. A frontier pair that is opened now has its first-pass value and
+// estimate subtracted (queued with a negative squared separation, evaluated
+// at the one far-field call site, so the value is the one the first pass
+// added) and is then exact or split like any pair.
+constexpr int kFrontFlag = int(0x80000000u);
+template <bool kLearn, bool kRecord, int kMode>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
+  constexpr bool kFront = kMode == 1, kCont = kMode == 2;
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
-  __shared__ float4 s_farv[kWarps][64];  // separation (x, y, z) and its square, per queued far pair
+  __shared__ float4 s_farv[kWarps][64];  // separation (x, y, z) and its square (negative: subtract), per queued far pair
   __shared__ float2 s_farr[kWarps][64];  // the two radii
   __shared__ std::conditional_t<kLearn, MlpFrag, int> s_mlp;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -969,7 +981,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     __syncthreads();
   }
   int2 *spill = A.spill + (size_t)gw * kSpill;
-  double nfar = 0, nent = 0;
+  double nfar = 0, nent = 0, nreuse = 0, nsub = 0;
   long long frec = -1;  // open frontier record (kFront)
   int ffill = 0, fslot = -1;
   const long long total = A.nin + A.nin1;
@@ -985,7 +997,8 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     if (b >= total) break;
     int slot, cnt0;
     const int2 *src;
-    if (b < A.nin) {
+    const bool from_front = b >= A.nin;
+    if (!from_front) {
       slot = A.in[b].slot;
       cnt0 = A.in[b].count;
       src = A.in[b].pairs;
@@ -1006,14 +1019,18 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     const double itolsq = A.itolsq[slot], eps = A.epssq;
     // Threshold of the learned criterion: tau x (beta0 / beta)^4 in later passes.
     const float log10_tau = A.learned.log10_tau + 2.f * (float)log10(A.beta0 * A.beta0 / itolsq);
-    for (int x = lane; x < cnt0; x += 32) stack[x] = src[x];
+    for (int x = lane; x < cnt0; x += 32) {
+      int2 v = src[x];
+      if (kCont && from_front) v.x |= kFrontFlag;
+      stack[x] = v;
+    }
     int top = cnt0, nspill = 0, nf = 0, steps = 0;
     long long bc = -1;  // open chunk of the exact list
     int bfill = 0;      // entries in it
     bool overflow = false;
     double sum = 0.0, err = 0.0;
     __syncwarp();
-    while (true) {
+    for (bool done = false; !done;) {
       if (top == 0 && nspill > 0) {  // refill from the spill buffer
         const int k = min(nspill, kStack / 2);
         for (int x = lane; x < k; x += 32) stack[x] = spill[nspill - k + x];
@@ -1021,210 +1038,229 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         top = k;
         __syncwarp();
       }
-      if (top == 0) break;
-      if (steps >= A.budget) {  // hand the rest on as new batches
-        const int total = top + nspill;
-        const int nb = (total + 31) / 32;
+      if (top == 0) done = true;
+      if (!done && steps >= A.budget) {  // hand the rest on as new batches
+        const int total_e = top + nspill;
+        const int nb = (total_e + 31) / 32;
         unsigned long long at = 0;
         if (lane == 0) at = atomicAdd(A.out_count, (unsigned long long)nb);
         at = __shfl_sync(0xffffffffu, at, 0);
         if ((long long)(at + nb) <= A.out_cap) {
           for (int q = 0; q < nb; ++q) {
             const int e = 32 * q + lane;
-            if (e < total) A.out[at + q].pairs[lane] = e < nspill ? spill[e] : stack[e - nspill];
+            if (e < total_e) A.out[at + q].pairs[lane] = e < nspill ? spill[e] : stack[e - nspill];
             if (lane == 0) {
               A.out[at + q].slot = slot;
-              A.out[at + q].count = min(32, total - 32 * q);
+              A.out[at + q].count = min(32, total_e - 32 * q);
             }
           }
           top = 0;
           nspill = 0;
           __syncwarp();
-          break;
-        }
-        // No room left: mark the reserved batches below the capacity empty
-        // and finish this batch here.
-        if (lane == 0)
-          for (int q = 0; q < nb && (long long)(at + q) < A.out_cap; ++q) {
-            A.out[at + q].slot = slot;
-            A.out[at + q].count = 0;
-          }
-        steps = INT_MIN;
-      }
-      ++steps;
-      const int cnt = min(top, 32);
-      const bool act = lane < cnt;
-      int2 pr = make_int2(0, 0);
-      if (act) pr = stack[top - cnt + lane];
-      __syncwarp();
-      top -= cnt;
-      int kind = 0;  // 0 none, 1 exact (leaf pair or bucket), 2 far, 3 split
-      int4 ex = make_int4(0, 0, 1, 1);
-      int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
-      float sep = 0.f;
-      double dsq = 0.0;
-      float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
-      float2 fr = make_float2(0.f, 0.f);
-      int mincnt = 0;  // segments of the smaller node (learned criterion)
-      if (act) {
-        const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
-        const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-        const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
-        const double rs = h1.r + h2.r;
-        dsq = dx * dx + dy * dy + dz * dz + eps;
-        fv = make_float4((float)dx, (float)dy, (float)dz, (float)dsq);
-        fr = make_float2((float)h1.r, (float)h2.r);
-        sep = (float)(sqrt(dsq) / rs);
-        if constexpr (kLearn) mincnt = min(h1.cnt, h2.cnt);
-        if (leaf1 && leaf2) {
-          kind = 1;
-          ex = make_int4(h1.lo, h2.lo, 1, 1);
-        } else if (dsq > rs * rs * itolsq + eps) {
-          kind = 2;
-        } else if (h1.cnt <= A.bucket && h2.cnt <= A.bucket) {
-          kind = 1;
-          ex = make_int4(h1.lo, h2.lo, h1.cnt, h2.cnt);
+          done = true;
         } else {
-          kind = 3;
-          const bool split2 = (!leaf1 && !leaf2) ? (h2.rsq > h1.rsq) : !leaf2;
-          if (split2) {
-            c0 = make_int2(pr.x, h2.left);
-            c1 = make_int2(pr.x, h2.right);
+          // No room left: mark the reserved batches below the capacity empty
+          // and finish this batch here.
+          if (lane == 0)
+            for (int q = 0; q < nb && (long long)(at + q) < A.out_cap; ++q) {
+              A.out[at + q].slot = slot;
+              A.out[at + q].count = 0;
+            }
+          steps = INT_MIN;
+        }
+      }
+      if (!done) {
+        ++steps;
+        const int cnt = min(top, 32);
+        const bool act = lane < cnt;
+        int2 pr = make_int2(0, 0);
+        if (act) pr = stack[top - cnt + lane];
+        __syncwarp();
+        top -= cnt;
+        bool fpair = false;  // a frontier pair of the continued retry
+        if constexpr (kCont) {
+          fpair = pr.x < 0;
+          pr.x &= ~kFrontFlag;
+        }
+        int kind = 0;  // 0 none, 1 exact (leaf pair or bucket), 2 far, 3 split
+        int4 ex = make_int4(0, 0, 1, 1);
+        int2 c0 = make_int2(0, 0), c1 = make_int2(0, 0);
+        float sep = 0.f;
+        double dsq = 0.0;
+        float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 fr = make_float2(0.f, 0.f);
+        int mincnt = 0;  // segments of the smaller node (learned criterion)
+        if (act) {
+          const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
+          const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+          const bool leaf1 = h1.left < 0, leaf2 = h2.left < 0;
+          const double rs = h1.r + h2.r;
+          dsq = dx * dx + dy * dy + dz * dz + eps;
+          fv = make_float4((float)dx, (float)dy, (float)dz, (float)dsq);
+          fr = make_float2((float)h1.r, (float)h2.r);
+          sep = (float)(sqrt(dsq) / rs);
+          if constexpr (kLearn) mincnt = min(h1.cnt, h2.cnt);
+          if (leaf1 && leaf2) {
+            kind = 1;
+            ex = make_int4(h1.lo, h2.lo, 1, 1);
+          } else if (dsq > rs * rs * itolsq + eps) {
+            kind = 2;
+          } else if (h1.cnt <= A.bucket && h2.cnt <= A.bucket) {
+            kind = 1;
+            ex = make_int4(h1.lo, h2.lo, h1.cnt, h2.cnt);
           } else {
-            c0 = make_int2(h1.left, pr.y);
-            c1 = make_int2(h1.right, pr.y);
+            kind = 3;
+            const bool split2 = (!leaf1 && !leaf2) ? (h2.rsq > h1.rsq) : !leaf2;
+            if (split2) {
+              c0 = make_int2(pr.x, h2.left);
+              c1 = make_int2(pr.x, h2.right);
+            } else {
+              c0 = make_int2(h1.left, pr.y);
+              c1 = make_int2(h1.right, pr.y);
+            }
           }
         }
-      }
-      // Recording for training: opened pairs and far pairs near the threshold.
-      if (kRecord && act && kind != 1 && sep >= A.rec_smin && sep * sep <= 1.5625f * (float)itolsq) {
-        uint32_t hsh = (uint32_t)slot * 0x9E3779B1u ^ (uint32_t)pr.x * 0x85EBCA77u ^ (uint32_t)pr.y * 0xC2B2AE3Du;
-        hsh ^= hsh >> 15;
-        hsh *= 0x2C1B3C6Du;
-        hsh ^= hsh >> 12;
-        if (hsh < A.rec_keep) {
-          const unsigned long long at = atomicAdd(A.rec_count, 1ULL);
-          if ((int64_t)at < A.rec_cap) A.rec[at] = make_int4(slot, pr.x, pr.y, 0);
-        }
-      }
-      // Learned criterion: a pair the beta test opens but whose separation is
-      // at least s_min is accepted as far-field when the MLP predicts its
-      // error below tau; it then adds its Eq. 14 estimate to err like any
-      // far-field pair. The warp's candidates are evaluated at once, and only
-      // when there are at least min_cand (>= 1) of them.
-      if constexpr (kLearn) {
-        const bool cand = kind == 3 && sep >= A.learned.s_min && mincnt >= A.learned.min_seg;
-        if (__popc(__ballot_sync(0xffffffffu, cand)) >= A.learned.min_cand) {
-          float f[kMlpIn];
-          for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
-          if (cand) {
-            const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
-            const NodeMom &ma = M1[pr.x], &mb = M2[pr.y];
-            mlp_features(sep, (float)h1.r, (float)h2.r, dsq, ma.tn, mb.tn, ma.dn, mb.dn, ma.qn, mb.qn, f);
+        // Recording for training: opened pairs and far pairs near the threshold.
+        if (kRecord && act && kind != 1 && sep >= A.rec_smin && sep * sep <= 1.5625f * (float)itolsq) {
+          uint32_t hsh = (uint32_t)slot * 0x9E3779B1u ^ (uint32_t)pr.x * 0x85EBCA77u ^ (uint32_t)pr.y * 0xC2B2AE3Du;
+          hsh ^= hsh >> 15;
+          hsh *= 0x2C1B3C6Du;
+          hsh ^= hsh >> 12;
+          if (hsh < A.rec_keep) {
+            const unsigned long long at = atomicAdd(A.rec_count, 1ULL);
+            if ((int64_t)at < A.rec_cap) A.rec[at] = make_int4(slot, pr.x, pr.y, 0);
           }
-          const float y = mlp_warp_predict(reinterpret_cast<const MlpFrag &>(s_mlp), f);
-          if (cand && y < log10_tau) kind = 2;
         }
-      }
-      const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
-      const int ns = __popc(sm);
-      if (top + 2 * ns > kStack) {  // spill the oldest half
-        const int k = top / 2;
-        if (nspill + k > A.spill_cap) {
-          overflow = true;
-          break;
+        // Learned criterion: a pair the beta test opens but whose separation is
+        // at least s_min is accepted as far-field when the MLP predicts its
+        // error below tau; it then adds its Eq. 14 estimate to err like any
+        // far-field pair. The warp's candidates are evaluated at once, and only
+        // when there are at least min_cand (>= 1) of them.
+        if constexpr (kLearn) {
+          const bool cand = kind == 3 && sep >= A.learned.s_min && mincnt >= A.learned.min_seg;
+          if (__popc(__ballot_sync(0xffffffffu, cand)) >= A.learned.min_cand) {
+            float f[kMlpIn];
+            for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+            if (cand) {
+              const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
+              const NodeMom &ma = M1[pr.x], &mb = M2[pr.y];
+              mlp_features(sep, (float)h1.r, (float)h2.r, dsq, ma.tn, mb.tn, ma.dn, mb.dn, ma.qn, mb.qn, f);
+            }
+            const float y = mlp_warp_predict(reinterpret_cast<const MlpFrag &>(s_mlp), f);
+            if (cand && y < log10_tau) kind = 2;
+          }
         }
-        for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
-        __syncwarp();
-        shift_down(stack, k, top - k, lane);
-        nspill += k;
-        top -= k;
-        __syncwarp();
-      }
-      if (kind == 3) {
-        const int rank = __popc(sm & ((1u << lane) - 1));
-        stack[top + 2 * rank] = c0;
-        stack[top + 2 * rank + 1] = c1;
-      }
-      top += 2 * ns;
-      const unsigned fm = __ballot_sync(0xffffffffu, kind == 2);
-      const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
-      if (kind == 2) {
-        const int at = nf + __popc(fm & ((1u << lane) - 1));
-        farq[at] = pr;
-        farv[at] = fv;
-        farr[at] = fr;
-      }
+        // Continued retry: a frontier pair still far keeps its first-pass
+        // value; one that opens gives it back (subtract) and goes on.
+        bool sub = false;
+        if constexpr (kCont) {
+          if (fpair) {
+            if (kind == 2) {
+              kind = 0;
+              nreuse += 1;
+            } else {
+              sub = true;
+              nsub += 1;
+              fv.w = -fv.w;
+            }
+          }
+        }
+        const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
+        const int ns = __popc(sm);
+        if (top + 2 * ns > kStack) {  // spill the oldest half
+          const int k = top / 2;
+          if (nspill + k > A.spill_cap) {
+            overflow = true;
+            done = true;
+          } else {
+            for (int x = lane; x < k; x += 32) spill[nspill + x] = stack[x];
+            __syncwarp();
+            shift_down(stack, k, top - k, lane);
+            nspill += k;
+            top -= k;
+            __syncwarp();
+          }
+        }
+        if (!overflow) {
+          if (kind == 3) {
+            const int rank = __popc(sm & ((1u << lane) - 1));
+            stack[top + 2 * rank] = c0;
+            stack[top + 2 * rank + 1] = c1;
+          }
+          top += 2 * ns;
+          const unsigned fm = __ballot_sync(0xffffffffu, kind == 2 || sub);
+          const unsigned lm = __ballot_sync(0xffffffffu, kind == 1);
+          if (kind == 2 || sub) {
+            const int at = nf + __popc(fm & ((1u << lane) - 1));
+            farq[at] = pr;
+            farv[at] = fv;
+            farr[at] = fr;
+          }
 #if FLN_BH_PREFETCH & 2
-      if (kind == 2) {
-        prefetch_record(M1 + pr.x);
-        prefetch_record(M2 + pr.y);
-      }
-#endif
-      nf += __popc(fm);
-      if (lm) {  // append the exact pairs to the list, 32 entries per chunk
-        const int ne = __popc(lm), pos = bfill + __popc(lm & ((1u << lane) - 1));
-        nent += ne;
-        const int need = (bc < 0 ? 1 : 0) + (bfill + ne > 32 ? 1 : 0);
-        long long c = 0;
-        if (lane == 0 && need) c = (long long)atomicAdd(A.bkt_count, (unsigned long long)need);
-        c = __shfl_sync(0xffffffffu, c, 0);
-        const long long cur = bc < 0 ? c : bc, nxt = bc < 0 ? c + 1 : c;
-        const long long dst = pos < 32 ? cur : nxt;
-        if (kind == 1) {
-          if (dst < A.bkt_cap) A.bkt[dst].e[pos & 31] = ex;
-          else atomicOr(A.status, 4);
-        }
-        if (bfill + ne >= 32) {
-          if (lane == 0 && cur < A.bkt_cap) {
-            A.bkt[cur].slot = slot;
-            A.bkt[cur].count = 32;
+          if (kind == 2 || sub) {
+            prefetch_record(M1 + pr.x);
+            prefetch_record(M2 + pr.y);
           }
-          bc = bfill + ne > 32 ? nxt : -1;
-          bfill = bfill + ne - 32;
-        } else {
-          bc = cur;
-          bfill += ne;
-        }
-      }
-      __syncwarp();
-#if FLN_BH_PREFETCH & 1
-      {  // the next step's headers, while the queued evaluations run
-        const int nxt = min(top, 32);
-        if (lane < nxt) {
-          const int2 p = stack[top - nxt + lane];
-          prefetch_record(H1 + p.x);
-          prefetch_record(H2 + p.y);
-        }
-      }
 #endif
-      while (nf >= 32) {
-        const int2 q = farq[nf - 32 + lane];
-        const float4 v = farv[nf - 32 + lane];
-        const float2 rr = farr[nf - 32 + lane];
-        if constexpr (kFront) front_put(A, frec, ffill, slot, q, 32, lane);
-        far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)v.w, rr.x, rr.y, sum, err);
-        nfar += 32;
-        nf -= 32;
+          nf += __popc(fm);
+          if (lm) {  // append the exact pairs to the list, 32 entries per chunk
+            const int ne = __popc(lm), pos = bfill + __popc(lm & ((1u << lane) - 1));
+            nent += ne;
+            const int need = (bc < 0 ? 1 : 0) + (bfill + ne > 32 ? 1 : 0);
+            long long c = 0;
+            if (lane == 0 && need) c = (long long)atomicAdd(A.bkt_count, (unsigned long long)need);
+            c = __shfl_sync(0xffffffffu, c, 0);
+            const long long cur = bc < 0 ? c : bc, nxt = bc < 0 ? c + 1 : c;
+            const long long dst = pos < 32 ? cur : nxt;
+            if (kind == 1) {
+              if (dst < A.bkt_cap) A.bkt[dst].e[pos & 31] = ex;
+              else atomicOr(A.status, 4);
+            }
+            if (bfill + ne >= 32) {
+              if (lane == 0 && cur < A.bkt_cap) {
+                A.bkt[cur].slot = slot;
+                A.bkt[cur].count = 32;
+              }
+              bc = bfill + ne > 32 ? nxt : -1;
+              bfill = bfill + ne - 32;
+            } else {
+              bc = cur;
+              bfill += ne;
+            }
+          }
+          __syncwarp();
+        }
+      }
+      // Far-field evaluation, 32 queued pairs at a time, and what is left
+      // once the batch is done: the one far-field call site of the kernel
+      // (a subtraction then gives back exactly what the first pass added).
+      while (nf >= 32 || (done && nf > 0)) {
+        const int m = min(nf, 32);
+        int2 q = make_int2(0, 0);
+        if (lane < m) q = farq[nf - m + lane];
+        if constexpr (kFront) front_put(A, frec, ffill, slot, q, m, lane);
+        if (lane < m) {
+          const float4 v = farv[nf - m + lane];
+          const float2 rr = farr[nf - m + lane];
+          double fs = 0.0, fe = 0.0;
+          far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)fabsf(v.w), rr.x, rr.y, fs, fe);
+          if (v.w < 0.f) {
+            sum -= fs;
+            err -= fe;
+          } else {
+            sum += fs;
+            err += fe;
+            nfar += 1;
+          }
+        }
+        nf -= m;
         __syncwarp();
       }
-    }
-    // Evaluate what is still queued.
-    if constexpr (kFront) {
-      if (nf > 0) front_put(A, frec, ffill, slot, lane < nf ? farq[lane] : make_int2(0, 0), nf, lane);
-    }
-    if (lane < nf) {
-      const int2 q = farq[lane];
-      const float4 v = farv[lane];
-      const float2 rr = farr[lane];
-      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)v.w, rr.x, rr.y, sum, err);
     }
     if (bc >= 0 && lane == 0 && bc < A.bkt_cap) {
       A.bkt[bc].slot = slot;
       A.bkt[bc].count = bfill;
     }
-    nfar += nf;
-    __syncwarp();
     if (overflow && lane == 0) atomicExch(A.status, 1);
     for (int o = 16; o; o >>= 1) {
       sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -1236,9 +1272,20 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     }
   }
   if constexpr (kFront) front_close(A, frec, ffill, fslot, lane);
+  for (int o = 16; o; o >>= 1) {
+    nfar += __shfl_xor_sync(0xffffffffu, nfar, o);
+    if constexpr (kCont) {
+      nreuse += __shfl_xor_sync(0xffffffffu, nreuse, o);
+      nsub += __shfl_xor_sync(0xffffffffu, nsub, o);
+    }
+  }
   if (lane == 0) {
     atomicAdd(A.counts, nfar);
     atomicAdd(A.counts + 5, nent);
+    if constexpr (kCont) {
+      atomicAdd(A.counts + 6, nreuse);
+      atomicAdd(A.counts + 7, nsub);
+    }
   }
 }
 
@@ -1500,12 +1547,14 @@ __global__ void __launch_bounds__(32 * kBkWarps, FLN_BUCKET_MIN_CTAS) bh_buckets
   if (lane == 0 && nexact > 0) atomicAdd(A.counts + 1, nexact);
 }
 
-// (Without a minimum CTA count: ptxas then settles at 96 registers, five CTAs
-// per SM; a minimum of 1 let it take 138.)
-__global__ void __launch_bounds__(32 * kWarps) bh_traverse(TravArgs A) { traverse<false, false, false>(A); }
+// Five CTAs per SM (at most 102 registers; without a minimum CTA count a
+// minimum of 1 is assumed and ptxas took up to 138).
+__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse(TravArgs A) { traverse<false, false, 0>(A); }
 // The first pass, which records its frontier for the beta retry.
-__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_front(TravArgs A) { traverse<false, false, true>(A); }
-__global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, false>(A); }
+__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_front(TravArgs A) { traverse<false, false, 1>(A); }
+// The beta retry continued from the first pass's frontier.
+__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_cont(TravArgs A) { traverse<false, false, 2>(A); }
+__global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, 0>(A); }
 // The learned kernels at FLN_LEARNED_MIN_CTAS CTAs per SM: their MLP code
 // (BF16 warp MMA) takes 168 registers at three CTAs; held to five, the
 // traversal keeps the plain kernel's occupancy and the inference, which runs
@@ -1514,10 +1563,13 @@ __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { 
 #define FLN_LEARNED_MIN_CTAS 5
 #endif
 __global__ void __launch_bounds__(32 * kWarps, FLN_LEARNED_MIN_CTAS) bh_traverse_learned(TravArgs A) {
-  traverse<true, false, false>(A);
+  traverse<true, false, 0>(A);
 }
 __global__ void __launch_bounds__(32 * kWarps, FLN_LEARNED_MIN_CTAS) bh_traverse_learned_front(TravArgs A) {
-  traverse<true, false, true>(A);
+  traverse<true, false, 1>(A);
+}
+__global__ void __launch_bounds__(32 * kWarps, FLN_LEARNED_MIN_CTAS) bh_traverse_learned_cont(TravArgs A) {
+  traverse<true, false, 2>(A);
 }
 
 // ------------------------------------------------------------------ split evaluation
@@ -1791,16 +1843,6 @@ __global__ void root_batches(const int32_t *slots, int64_t n, const int32_t *slo
   acc_lk[s] = 0;
   acc_err[s] = 0;
   acc_exact[s] = 0;
-}
-
-// Slots whose beta retry continues from the first pass's frontier: the far
-// and error sums restart, the exact sum of the first pass stays.
-__global__ void continue_slots(const int32_t *slots, int64_t n, unsigned long long *acc_lk,
-                               unsigned long long *acc_err) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  acc_lk[slots[k]] = 0;
-  acc_err[slots[k]] = 0;
 }
 
 // Fixed-point sums (far-field + exact) -> per caller pair doubles.
@@ -2515,7 +2557,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_slots, slot_loops.data(), 2 * np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemcpyAsync(d_slot_pair, order.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
-  FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
+  FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, 3 * sizeof(double), st));  // exact entries, reused, subtracted
   const double b0 = prm.barnes_hut_init_beta;
   const int budget = prm.bh_budget > 0 ? prm.bh_budget : FLN_BH_BUDGET;
   // Buckets need contiguous segment ranges: curve-order trees only.
@@ -2566,6 +2608,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   // slots whose skip byte is 0. `front` records this pass's frontier.
   auto pass = [&](const std::vector<int32_t> &roots, const std::vector<double> &itol_slots, bool record, bool front,
                   int64_t nstream) {
+    const bool cont = nstream > 0;  // the retry continued from the frontier
     const int64_t na = (int64_t)roots.size();
     FLN_CUDA(cudaMemcpyAsync(d_active, roots.data(), na * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     FLN_CUDA(cudaMemcpyAsync(d_itol, itol_slots.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -2636,9 +2679,10 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       if (A.rec)
         bh_traverse_record<<<g, 32 * kWarps, 0, st>>>(A);
       else if (A.learned.frag)
-        (front ? bh_traverse_learned_front : bh_traverse_learned)<<<g, 32 * kWarps, 0, st>>>(A);
+        (front ? bh_traverse_learned_front : cont ? bh_traverse_learned_cont : bh_traverse_learned)
+            <<<g, 32 * kWarps, 0, st>>>(A);
       else
-        (front ? bh_traverse_front : bh_traverse)<<<g, 32 * kWarps, 0, st>>>(A);
+        (front ? bh_traverse_front : cont ? bh_traverse_cont : bh_traverse)<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
       BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc_exact, d_counts};
       FLN_CUDA(cudaEventRecord(ctx.ev_bk[0], st));
@@ -2739,7 +2783,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)bkt_cap * sizeof(BucketChunk)));
     d_status = reinterpret_cast<int32_t *>(d_counts + 2);
     FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
-    FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, sizeof(double), st));
+    FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, 3 * sizeof(double), st));
   }
   std::vector<int32_t> all(np);
   std::iota(all.begin(), all.end(), 0);
@@ -2778,15 +2822,16 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     }
   }
   ctx.stats.beta_retried = (int64_t)retry_slots.size();
-  std::vector<double> far_leaf(6, 0.0);
+  std::vector<double> far_leaf(8, 0.0);
   if (!retry_slots.empty()) {
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
     if (use_front && (status & 1) == 0) {
       // A node pair opened at beta0 is opened at beta* > beta0 (far at beta*
       // implies far at beta0), and an exact pair stays exact (the bucket test
       // does not depend on beta). So the beta* pass is the beta0 pass
-      // continued from its far node pairs: the exact sums stay, the far sums
-      // restart from the frontier. Slots whose frontier did not fit start
+      // continued from its far node pairs: the slot keeps its sums, the
+      // frontier pairs still far keep their values, the ones that open give
+      // theirs back (bh_traverse_cont). Slots whose frontier did not fit start
       // from the roots.
       std::vector<uint8_t> skip(np, 1);
       std::vector<int32_t> cont, from_roots;
@@ -2799,14 +2844,6 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         }
       }
       FLN_CUDA(cudaMemcpyAsync(d_skip, skip.data(), np, cudaMemcpyHostToDevice, st));
-      if (!cont.empty()) {
-        int32_t *d_cont = reinterpret_cast<int32_t *>(ctx.d_bh[24].need(cont.size() * sizeof(int32_t)));
-        FLN_CUDA(cudaMemcpyAsync(d_cont, cont.data(), cont.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-        continue_slots<<<(int)((cont.size() + 255) / 256), 256, 0, st>>>(d_cont, (int64_t)cont.size(), d_acc,
-                                                                           d_acc_err);
-        FLN_CUDA(cudaGetLastError());
-        ++launches;
-      }
       ctx.stats.bh_retry_from_roots = (int64_t)from_roots.size();
       pass(from_roots, itol, false, false, cont.empty() ? 0 : front_n);
     } else {
@@ -2865,13 +2902,15 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     ctx.stats.ms_retry += ms;
     for (int32_t s : up) err[order[s]] = e3[order[s]] * prm.error_est_scale;
   }
-  FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FLN_CUDA(cudaMemcpyAsync(far_leaf.data(), d_counts, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
   FLN_CUDA(cudaMemcpyAsync(d_err_out, err.data(), np * sizeof(double), cudaMemcpyHostToDevice, st));
   if (d_flags_out) FLN_CUDA(cudaMemcpyAsync(d_flags_out, flags.data(), np * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   FLN_CUDA(cudaStreamSynchronize(st));
   ctx.stats.bh_far_evals = far_leaf[0];
   ctx.stats.bh_leaf_evals = far_leaf[1];
   ctx.stats.bh_exact_entries = prm.bh_schedule == 0 ? far_leaf[5] : far_leaf[1];
+  ctx.stats.bh_far_reused = far_leaf[6];
+  ctx.stats.bh_far_subtracted = far_leaf[7];
   if (status & 1)
     throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
                                             std::to_string(maxdepth) + ").");

@@ -145,6 +145,7 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   ctx.stats.ms_retry = 0;
   ctx.stats.bh_front_records = ctx.stats.bh_retry_from_roots = 0;
   ctx.stats.bh_wait_timeouts = 0;
+  ctx.stats.bh_far_reused = ctx.stats.bh_far_subtracted = 0;
   ctx.stats.beta_retried = 0;
   ctx.stats.bh_escalated = 0;
   if (!d_err) d_err = ctx.d_err.as<double>(std::max<int64_t>(np, 1));  // Barnes–Hut needs one

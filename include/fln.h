@@ -147,7 +147,11 @@ typedef struct fln_stats {
                                    the first pass for the retry to continue from */
   int64_t bh_retry_from_roots;  /* Barnes–Hut: retried pairs that restarted from the roots (frontier not
                                    kept for them, or bh_retry_from_roots set) */
-  double reserved_stats2[4];
+  double bh_far_reused;         /* Barnes–Hut: frontier node pairs still far at the retry's beta, whose
+                                   first-pass values were kept (not evaluated again) */
+  double bh_far_subtracted;     /* Barnes–Hut: frontier node pairs opened by the retry, whose first-pass
+                                   values were given back */
+  double reserved_stats2[2];
 } fln_stats;
 
 typedef struct fln_ctx fln_ctx;

@@ -6,7 +6,9 @@ A node pair opened at beta0 is opened at beta* > beta0 (far at beta* implies
 far at beta0), and an exact node pair stays exact (the bucket test does not
 depend on beta), so the beta* traversal is the beta0 traversal continued from
 its far node pairs. The engine records those far pairs in its first pass and
-continues from them (bh_retry_from_roots = 0, the default).
+continues from them (bh_retry_from_roots = 0, the default): a frontier pair
+still far at beta* keeps its first-pass value (a far-field value does not
+depend on beta), one that opens gives its value back and is traversed.
 
 Checked against the oracle's restatement (curve_bh_eval_continued: the
 continued pass node pair for node pair, sums within 2e-5 as the one-pass
@@ -64,10 +66,13 @@ def test_continued_retry_matches_oracle(engine, case, beta1, golden_dir):
     assert s["bh_retry_from_roots"] == 0 and s["bh_front_records"] > 0
     np.testing.assert_allclose(lk, np.where(retried, lk1_o, lk0_o), rtol=0, atol=2e-5)
     np.testing.assert_allclose(err, np.where(retried, err1_o, err0_o), rtol=1e-3, atol=1e-9)
+    # Frontier pairs still far at beta1 keep their first-pass values and are
+    # not evaluated again: evaluated + kept = the oracle's far pairs.
     far_total = float(far0_o.sum() + far1_o[retried].sum())
     ex_total = float(np.where(retried, ex1_o, ex0_o).sum())
-    assert abs(s["bh_far_evals"] - far_total) <= 1e-5 * far_total + 2
+    assert abs(s["bh_far_evals"] + s["bh_far_reused"] - far_total) <= 1e-5 * far_total + 2
     assert abs(s["bh_leaf_evals"] - ex_total) <= 1e-5 * ex_total + 64
+    assert s["bh_far_reused"] > 0 and s["bh_far_subtracted"] > 0
 
 
 @pytest.mark.parametrize("case", ["polymer", "mixed"])
@@ -89,8 +94,10 @@ def test_continued_retry_equals_retry_from_roots(engine, case):
     np.testing.assert_allclose(lk_c, lk_r, rtol=0, atol=1e-8)
     np.testing.assert_allclose(err_c, err_r, rtol=1e-6, atol=1e-12)
     # The continuation evaluates fewer node pairs: the first pass's exact
-    # terms and opened node pairs are not visited again.
+    # terms, its opened node pairs and its far pairs that stay far are not
+    # evaluated again.
     assert s_c["bh_far_evals"] < s_r["bh_far_evals"] and s_c["bh_leaf_evals"] < s_r["bh_leaf_evals"]
+    assert s_c["bh_far_reused"] > 0 and s_r["bh_far_reused"] == 0
     print(f"{case}: retried {s_c['beta_retried']} of {len(pairs)}, retry {s_c['ms_retry']:.2f} ms "
           f"(from roots {s_r['ms_retry']:.2f} ms), far {s_c['bh_far_evals']:.3g} vs {s_r['bh_far_evals']:.3g}")
 
