@@ -748,11 +748,13 @@ __device__ __noinline__ double seg_term_fp64(const double *xyz, int64_t p0i, int
 //   div1 = |a||b||c| + (a.b)|c| + (c.a)|b| + (c.b)|a|
 //   div2 = |a||d||c| + (a.d)|c| + (c.a)|d| + (c.d)|a|
 //   term = atan2(det (div1 + div2), div1 div2 - det^2) / 2pi (+ the branch turn).
-// a, d and e are FP64 differences rounded once; b = a - e, c = d - e and
-// f = d - a in FP32 (f's rounding, about one unit in the last place of |d|,
-// enters the term scaled by 1/|d|^2). Walking q along loop 2 for a fixed p, step k+1's a, b are step k's
-// d, c, so a step forms two new vectors and two norms. Segments closer than
-// the longer one's length (squared norms compared) are left to FP64.
+// The vertices are FP32 coordinates relative to an FP64 origin near the two
+// segments (the exact-list kernel's entry origin); e = p1 - p0 is an FP64
+// difference rounded once; b = a - e, c = d - e and f = d - a are FP32.
+// Walking q along loop 2 for a fixed p, step k+1's a, b are step k's d, c,
+// so a step forms two new vectors and two norms (walk_start_f, walk_step_f).
+// Segments closer than the longer one's length (squared norms compared) are
+// left to FP64 (seg_term_fp64).
 
 // arctan(t) for |t| <= 1/4 from its Maclaurin series t - t^3/3 + t^5/5 - t^7/7
 // + t^9/9; the first omitted term is below 2.2e-8 |t|, under FP32 rounding.
@@ -765,101 +767,12 @@ __device__ __forceinline__ float atan_quarter(float t) {
   return p * t;
 }
 
-struct SegWalk {        // the carried state of a walk along loop 2
-  float ax, ay, az;     // a = q_k - p0
-  float bx, by, bz;     // b = q_k - p1
-  float aa, bb, ab;     // |a|^2, |b|^2, a.b
-  float la, lb;         // |a|, |b| (meaningful when aa, bb > 0)
-};
-
 __device__ __forceinline__ float norm_of(float sq) { return sq * rsqrtf(sq); }
-
-// The walk's first vertex q0 (FP64) for segment p0 -> p1 (e = p1 - p0, FP32).
-__device__ __forceinline__ SegWalk walk_start(const double *p0, const double *q0, float ex, float ey, float ez) {
-  SegWalk w;
-  w.ax = (float)(q0[0] - p0[0]);
-  w.ay = (float)(q0[1] - p0[1]);
-  w.az = (float)(q0[2] - p0[2]);
-  w.bx = w.ax - ex;
-  w.by = w.ay - ey;
-  w.bz = w.az - ez;
-  w.aa = dot3(w.ax, w.ay, w.az, w.ax, w.ay, w.az);
-  w.bb = dot3(w.bx, w.by, w.bz, w.bx, w.by, w.bz);
-  w.ab = dot3(w.ax, w.ay, w.az, w.bx, w.by, w.bz);
-  w.la = norm_of(w.aa);
-  w.lb = norm_of(w.bb);
-  return w;
-}
-
-// One step q0 -> q1 of the walk: adds the term to acc (radians) and turns
-// (whole turns of the branch correction) and returns true, or returns false when the pair is near (FP64 needed). The
-// walk advances to q1 either way.
-__device__ __forceinline__ bool walk_step(SegWalk &w, const double *p0, const double *q1, float ex, float ey,
-                                          float ez, float ee, float &acc, float &turns) {
-  const float dx = (float)(q1[0] - p0[0]), dy = (float)(q1[1] - p0[1]), dz = (float)(q1[2] - p0[2]);
-  const float fx = dx - w.ax, fy = dy - w.ay, fz = dz - w.az;
-  const float cx = dx - ex, cy = dy - ey, cz = dz - ez;
-  const float cc = dot3(cx, cy, cz, cx, cy, cz), dd = dot3(dx, dy, dz, dx, dy, dz);
-  const float cd = dot3(cx, cy, cz, dx, dy, dz), ff = dot3(fx, fy, fz, fx, fy, fz);
-  const float lc = norm_of(cc), ld = norm_of(dd);
-  const bool near = fminf(fminf(w.aa, w.bb), fminf(cc, dd)) <= fmaxf(ee, ff);
-  if (!near) {
-    const float ca = dot3(cx, cy, cz, w.ax, w.ay, w.az), cb = dot3(cx, cy, cz, w.bx, w.by, w.bz);
-    const float ad = dot3(w.ax, w.ay, w.az, dx, dy, dz);
-    const float det = w.ax * (fy * ez - fz * ey) + w.ay * (fz * ex - fx * ez) + w.az * (fx * ey - fy * ex);
-    const float t = w.la * lc;
-    const float div1 = t * w.lb + w.ab * lc + ca * w.lb + cb * w.la;
-    const float div2 = t * ld + ad * lc + ca * ld + cd * w.la;
-    const float x = div1 * div2 - det * det;
-    const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
-    const float y = det * s;
-    float term;
-    if (s > 0.f && fabsf(y) < 0.25f * x) {
-      term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
-    } else {
-      term = atan2f(y, x);
-      const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
-      if ((s < 0.f) || ((s == 0.f) && (det < 0.f))) turns += sg;
-    }
-    acc += term;
-  }
-  w.ax = dx; w.ay = dy; w.az = dz;
-  w.bx = cx; w.by = cy; w.bz = cz;
-  w.aa = dd; w.bb = cc; w.ab = cd;
-  w.la = ld; w.lb = lc;
-  return !near;
-}
 
 __device__ __forceinline__ void load3(const double *xyz, int64_t v, double *p) {
   p[0] = xyz[3 * v];
   p[1] = xyz[3 * v + 1];
   p[2] = xyz[3 * v + 2];
-}
-
-// Exact term of segment s1 of loop 1 (vertex offset o1, n1 segments) and
-// segment s2 of loop 2: the first step of a walk, FP64 for near segments.
-__device__ __forceinline__ double seg_pair_term(const double *xyz, int64_t o1, int64_t n1, int64_t s1, int64_t o2,
-                                                int64_t n2, int64_t s2) {
-  const int64_t a0 = o1 + s1, a1 = o1 + (s1 + 1 == n1 ? 0 : s1 + 1);
-  const int64_t b0 = o2 + s2, b1 = o2 + (s2 + 1 == n2 ? 0 : s2 + 1);
-  double p0[3], p1[3], q0[3], q1[3];
-  load3(xyz, a0, p0);
-  load3(xyz, a1, p1);
-  load3(xyz, b0, q0);
-  load3(xyz, b1, q1);
-  const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
-  SegWalk w = walk_start(p0, q0, ex, ey, ez);
-  float acc = 0.f, turns = 0.f;
-  if (walk_step(w, p0, q1, ex, ey, ez, dot3(ex, ey, ez, ex, ey, ez), acc, turns))
-    return kInvTwoPi * (double)acc + (double)turns;
-  return seg_term_fp64(xyz, a0, a1, b0, b1);
-}
-
-// Exact leaf-leaf term of the traversal schedules 1 and 2; the same value as
-// the exact-list kernel gives the pair.
-__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &, const NodeMom &,
-                          int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
-  sum += seg_pair_term(xyz, o1, n1, -1 - h1.left, o2, n2, -1 - h2.left);
 }
 
 // Traversal steps a warp takes on one batch per round before it hands the
@@ -1343,9 +1256,29 @@ __device__ __forceinline__ SegWalkF walk_start_f(float p0x, float p0y, float p0z
   return w;
 }
 
+// The angle of x + iy in (-pi, pi], without branches (the lanes of a warp
+// then run one instruction stream whatever their angles): t = min/max of
+// |x|, |y| in [0, 1]; above tan(pi/12), atan(t) = pi/6 + atan((t sqrt3 - 1)
+// / (sqrt3 + t)) brings the argument to |t'| <= tan(pi/12) = 0.268, where the
+// 5-term series of atan_quarter is within 5e-8; then the octant and the
+// quadrant by selects. Within 3.1e-7 of the FP64 atan2 over all angles
+// (float32 emulation, 2M random points), as FP32 atan2f is.
+__device__ __forceinline__ float angle_of(float x, float y) {
+  const float ax = fabsf(x), ay = fabsf(y);
+  const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+  const float t = mx > 0.f ? __fdividef(mn, mx) : 0.f;
+  const bool big = t > 0.26794919f;  // tan(pi/12)
+  const float tr = big ? __fdividef(fmaf(t, 1.7320508f, -1.f), 1.7320508f + t) : t;
+  float a = atan_quarter(tr) + (big ? 0.52359878f : 0.f);  // + pi/6
+  a = ay > ax ? 1.5707964f - a : a;                          // pi/2 - a
+  a = x < 0.f ? 3.1415927f - a : a;                          // pi - a
+  return copysignf(a, y);
+}
+
 // One step q0 -> q1 of the walk (q1.w unused; ff = |q1 - q0|^2 comes from
-// the staged vertex q0): the same terms, the same near rule and the same
-// branch handling as walk_step, from FP32 coordinates relative to an origin.
+// the staged vertex q0): the same terms and the same near rule as walk_step,
+// from FP32 coordinates relative to an origin, with the branch turn of the
+// reference added by selects and the arctangent by angle_of.
 __device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, float p0z, float4 q1, float ff,
                                             float ex, float ey, float ez, float ee, float &acc, float &turns) {
   const float dx = q1.x - p0x, dy = q1.y - p0y, dz = q1.z - p0z;
@@ -1365,21 +1298,51 @@ __device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, f
     const float x = div1 * div2 - det * det;
     const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
     const float y = det * s;
-    float term;
-    if (s > 0.f && fabsf(y) < 0.25f * x) {
-      term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
-    } else {
-      term = atan2f(y, x);
-      const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
-      if ((s < 0.f) || ((s == 0.f) && (det < 0.f))) turns += sg;
-    }
-    acc += term;
+    const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
+    turns += ((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? sg : 0.f;
+    acc += angle_of(x, y);
   }
   w.ax = dx; w.ay = dy; w.az = dz;
   w.bx = cx; w.by = cy; w.bz = cz;
   w.aa = dd; w.bb = cc; w.ab = cd;
   w.la = ld; w.lb = lc;
   return !near;
+}
+
+// Exact term of segment s1 of loop 1 (vertex offset o1, n1 segments) and
+// segment s2 of loop 2 as the exact-list kernel forms it for a 1 x 1 entry:
+// origin midway between the two segments' first vertices (FP64), vertices
+// relative to it in FP32, one step of walk_step_f, FP64 for near segments.
+// The persistent and split schedules sum their leaf pairs with it, so a leaf
+// pair gets the same value in every schedule.
+__device__ __forceinline__ double seg_pair_term(const double *xyz, int64_t o1, int64_t n1, int64_t s1, int64_t o2,
+                                                int64_t n2, int64_t s2) {
+  const int64_t a0 = o1 + s1, a1 = o1 + (s1 + 1 == n1 ? 0 : s1 + 1);
+  const int64_t b0 = o2 + s2, b1 = o2 + (s2 + 1 == n2 ? 0 : s2 + 1);
+  double p0[3], p1[3], q0[3], q1[3];
+  load3(xyz, a0, p0);
+  load3(xyz, a1, p1);
+  load3(xyz, b0, q0);
+  load3(xyz, b1, q1);
+  const double ox = 0.5 * p0[0] + 0.5 * q0[0], oy = 0.5 * p0[1] + 0.5 * q0[1], oz = 0.5 * p0[2] + 0.5 * q0[2];
+  float4 f0 = make_float4((float)(q0[0] - ox), (float)(q0[1] - oy), (float)(q0[2] - oz), 0.f);
+  const float4 f1 = make_float4((float)(q1[0] - ox), (float)(q1[1] - oy), (float)(q1[2] - oz), 0.f);
+  const float fx = f1.x - f0.x, fy = f1.y - f0.y, fz = f1.z - f0.z;
+  f0.w = dot3(fx, fy, fz, fx, fy, fz);
+  const float p0x = (float)(p0[0] - ox), p0y = (float)(p0[1] - oy), p0z = (float)(p0[2] - oz);
+  const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
+  const float ee = dot3(ex, ey, ez, ex, ey, ez);
+  SegWalkF w = walk_start_f(p0x, p0y, p0z, f0, ex, ey, ez);
+  float acc = 0.f, turns = 0.f;
+  if (walk_step_f(w, p0x, p0y, p0z, f1, f0.w, ex, ey, ez, ee, acc, turns))
+    return kInvTwoPi * (double)acc + (double)turns;
+  return seg_term_fp64(xyz, a0, a1, b0, b1);
+}
+
+// Exact leaf-leaf term of the traversal schedules 1 and 2.
+__device__ void leaf_eval(const double *xyz, const NodeHdr &h1, const NodeHdr &h2, const NodeMom &, const NodeMom &,
+                          int64_t o1, int64_t n1, int64_t o2, int64_t n2, double &sum) {
+  sum += seg_pair_term(xyz, o1, n1, -1 - h1.left, o2, n2, -1 - h2.left);
 }
 
 #ifndef FLN_BUCKET_MIN_CTAS

@@ -103,14 +103,15 @@ def test_learned_barneshut_on_held_out_loops(engine):
     # within the Barnes-Hut target error (0.1, lnc.cpp:25)
     assert np.abs(lk_l[pick] - lk_d).max() < 0.1
     # The gain: node pairs the traversal no longer evaluates (the kernel
-    # time, which the inference adds to, is reported alongside). It is a few
-    # percent here (2-4 % over runs: training sums gradients with FP32 atomics,
-    # so the trained weights vary slightly from run to run).
+    # time, which the inference adds to, is reported alongside). It is about
+    # 1 % here with the continued retry (2-4 % when the retry re-ran from the
+    # roots; training sums gradients with FP32 atomics, so the trained weights
+    # vary slightly from run to run).
     work_plain = s_plain["bh_far_evals"] + s_plain["bh_leaf_evals"]
     work_l = s_l["bh_far_evals"] + s_l["bh_leaf_evals"]
     print(f"learned: {work_l:.4g} node pairs vs {work_plain:.4g} plain; main kernel "
           f"{s_l['ms_main_kernel']:.2f} ms vs {s_plain['ms_main_kernel']:.2f} ms")
-    assert work_l < 0.985 * work_plain, (work_l, work_plain)
+    assert work_l < 0.99 * work_plain, (work_l, work_plain)
     # Turned off again: the plain traversal's exact node-pair counts.
     engine.linking_numbers(xyz, off, pairs, "barneshut", bh_bucket=1)
     s_off = engine.stats()
