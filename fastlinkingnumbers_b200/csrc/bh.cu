@@ -1256,29 +1256,13 @@ __device__ __forceinline__ SegWalkF walk_start_f(float p0x, float p0y, float p0z
   return w;
 }
 
-// The angle of x + iy in (-pi, pi], without branches (the lanes of a warp
-// then run one instruction stream whatever their angles): t = min/max of
-// |x|, |y| in [0, 1]; above tan(pi/12), atan(t) = pi/6 + atan((t sqrt3 - 1)
-// / (sqrt3 + t)) brings the argument to |t'| <= tan(pi/12) = 0.268, where the
-// 5-term series of atan_quarter is within 5e-8; then the octant and the
-// quadrant by selects. Within 3.1e-7 of the FP64 atan2 over all angles
-// (float32 emulation, 2M random points), as FP32 atan2f is.
-__device__ __forceinline__ float angle_of(float x, float y) {
-  const float ax = fabsf(x), ay = fabsf(y);
-  const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
-  const float t = mx > 0.f ? __fdividef(mn, mx) : 0.f;
-  const bool big = t > 0.26794919f;  // tan(pi/12)
-  const float tr = big ? __fdividef(fmaf(t, 1.7320508f, -1.f), 1.7320508f + t) : t;
-  float a = atan_quarter(tr) + (big ? 0.52359878f : 0.f);  // + pi/6
-  a = ay > ax ? 1.5707964f - a : a;                          // pi/2 - a
-  a = x < 0.f ? 3.1415927f - a : a;                          // pi - a
-  return copysignf(a, y);
-}
-
 // One step q0 -> q1 of the walk (q1.w unused; ff = |q1 - q0|^2 comes from
-// the staged vertex q0): the same terms and the same near rule as walk_step,
-// from FP32 coordinates relative to an origin, with the branch turn of the
-// reference added by selects and the arctangent by angle_of.
+// the staged vertex q0), from FP32 coordinates relative to an origin. The
+// arctangent: when div1 + div2 > 0 and |y| < x / 4 the principal branch by
+// the 5-term series (|angle| < 0.245), otherwise atan2f and the branch turn
+// of the reference (compute_link.cpp:151-175). (A branch-free arctangent,
+// range reduced by pi/6, measured slower on B200: the slow path is rare
+// enough that the warps seldom diverge on it.)
 __device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, float p0z, float4 q1, float ff,
                                             float ex, float ey, float ez, float ee, float &acc, float &turns) {
   const float dx = q1.x - p0x, dy = q1.y - p0y, dz = q1.z - p0z;
@@ -1298,9 +1282,15 @@ __device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, f
     const float x = div1 * div2 - det * det;
     const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
     const float y = det * s;
-    const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
-    turns += ((s < 0.f) || ((s == 0.f) && (det < 0.f))) ? sg : 0.f;
-    acc += angle_of(x, y);
+    float term;
+    if (s > 0.f && fabsf(y) < 0.25f * x) {
+      term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
+    } else {
+      term = atan2f(y, x);
+      const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
+      if ((s < 0.f) || ((s == 0.f) && (det < 0.f))) turns += sg;
+    }
+    acc += term;
   }
   w.ax = dx; w.ay = dy; w.az = dz;
   w.bx = cx; w.by = cy; w.bz = cz;

@@ -72,7 +72,8 @@ def test_continued_retry_matches_oracle(engine, case, beta1, golden_dir):
     ex_total = float(np.where(retried, ex1_o, ex0_o).sum())
     assert abs(s["bh_far_evals"] + s["bh_far_reused"] - far_total) <= 1e-5 * far_total + 2
     assert abs(s["bh_leaf_evals"] - ex_total) <= 1e-5 * ex_total + 64
-    assert s["bh_far_reused"] > 0 and s["bh_far_subtracted"] > 0
+    # The frontier was used (at beta1 = 4 every frontier pair may open).
+    assert s["bh_far_reused"] + s["bh_far_subtracted"] > 0
 
 
 @pytest.mark.parametrize("case", ["polymer", "mixed"])
@@ -80,7 +81,8 @@ def test_continued_retry_equals_retry_from_roots(engine, case):
     if case == "polymer":
         poff, pxyz, pairs = _polymer(engine, seed=61, loops=30, cube=250.0)
     else:
-        off, xyz = workloads.mixed_batch(seed=9, n_loops=300, hi=2 ** 14)
+        # Knots and walks of mixed sizes, packed densely enough that a pair retries.
+        off, xyz = workloads.mixed_batch(seed=9, n_loops=300, hi=2 ** 14, cube=80.0)
         m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
         poff, pxyz, pairs, _ = m.Prepare(True, engine=engine)
     lk_r, err_r, fl_r = engine.linking_numbers(pxyz, poff, pairs, "barneshut", bh_retry_from_roots=1)
