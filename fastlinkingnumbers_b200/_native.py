@@ -50,7 +50,7 @@ class TuneResult(C.Structure):
     _fields_ = [
         ("best_ms", C.c_double), ("default_ms", C.c_double), ("trials", C.c_int32),
         ("sample_pairs", C.c_int32), ("best_budget", C.c_int32), ("best_direct_tile", C.c_int32),
-        ("best_beta", C.c_double), ("best_bucket", C.c_int32), ("reserved1", C.c_int32),
+        ("best_beta", C.c_double), ("best_bucket", C.c_int32), ("best_occupancy", C.c_int32),
         ("reserved", C.c_double * 2),
     ]
 
@@ -69,7 +69,7 @@ class Params(C.Structure):
         ("bh_tree", C.c_int32), ("bh_escalations", C.c_int32), ("bh_err_limit", C.c_double),
         ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("bh_budget", C.c_int32),
         ("bh_bucket", C.c_int32), ("bh_retry_from_roots", C.c_int32), ("bh_spill_cap", C.c_int32),
-        ("bh_wait_polls", C.c_int64), ("direct_tile", C.c_int32), ("reserved_i0", C.c_int32),
+        ("bh_wait_polls", C.c_int64), ("direct_tile", C.c_int32), ("bh_occupancy", C.c_int32),
         ("reserved_params", C.c_double * 4),
     ]
 

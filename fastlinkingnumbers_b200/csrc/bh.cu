@@ -1500,13 +1500,33 @@ __global__ void __launch_bounds__(32 * kBkWarps, FLN_BUCKET_MIN_CTAS) bh_buckets
   if (lane == 0 && nexact > 0) atomicAdd(A.counts + 1, nexact);
 }
 
-// Five CTAs per SM (at most 102 registers; without a minimum CTA count a
-// minimum of 1 is assumed and ptxas took up to 138).
-__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse(TravArgs A) { traverse<false, false, 0>(A); }
-// The first pass, which records its frontier for the beta retry.
-__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_front(TravArgs A) { traverse<false, false, 1>(A); }
-// The beta retry continued from the first pass's frontier.
-__global__ void __launch_bounds__(32 * kWarps, 5) bh_traverse_cont(TravArgs A) { traverse<false, false, 2>(A); }
+// The traversal kernels at N CTAs per SM (fln_params.bh_occupancy): 5 (96
+// registers), 6 (80) or 7 (72, with some spills). The traversal is bound by
+// dependent loads, so more resident warps can pay for the spills. (Without a
+// minimum CTA count ptxas assumes one and took up to 138 registers.)
+//   bh_traverse_oN        plain
+//   bh_traverse_front_oN  the first pass, which records its frontier
+//   bh_traverse_cont_oN   the beta retry continued from that frontier
+#define FLN_TRAVERSE_KERNELS(N)                                                                              \
+  __global__ void __launch_bounds__(32 * kWarps, N) bh_traverse_o##N(TravArgs A) { traverse<false, false, 0>(A); } \
+  __global__ void __launch_bounds__(32 * kWarps, N) bh_traverse_front_o##N(TravArgs A) {                     \
+    traverse<false, false, 1>(A);                                                                            \
+  }                                                                                                          \
+  __global__ void __launch_bounds__(32 * kWarps, N) bh_traverse_cont_o##N(TravArgs A) {                      \
+    traverse<false, false, 2>(A);                                                                            \
+  }
+FLN_TRAVERSE_KERNELS(5)
+FLN_TRAVERSE_KERNELS(6)
+FLN_TRAVERSE_KERNELS(7)
+
+struct TraverseSet {
+  void (*plain)(TravArgs), (*front)(TravArgs), (*cont)(TravArgs);
+  int ctas;       // CTAs per SM the set is built for
+  int carveout;   // shared-memory carveout (percent) that fits that many CTAs of 15 KB
+};
+const TraverseSet kTraverseSets[] = {{bh_traverse_o5, bh_traverse_front_o5, bh_traverse_cont_o5, 5, FLN_BH_CARVEOUT},
+                                     {bh_traverse_o6, bh_traverse_front_o6, bh_traverse_cont_o6, 6, FLN_BH_CARVEOUT},
+                                     {bh_traverse_o7, bh_traverse_front_o7, bh_traverse_cont_o7, 7, 58}};
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, 0>(A); }
 // The learned kernels at FLN_LEARNED_MIN_CTAS CTAs per SM: their MLP code
 // (BF16 warp MMA) takes 168 registers at three CTAs; held to five, the
@@ -2485,14 +2505,17 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   unsigned long long *d_acc_exact = d_acc + 2 * np;
   // [0] queue, [1] next-round count, [2] exact (or far) chunks, [3] leaf chunks, [4] frontier records
   unsigned long long *d_ctr = d_acc + 3 * np;
-  int per_sm = 0, per_sm_f = 0;
-  FLN_CUDA(cudaFuncSetAttribute(bh_traverse, cudaFuncAttributePreferredSharedMemoryCarveout, FLN_BH_CARVEOUT));
-  FLN_CUDA(cudaFuncSetAttribute(bh_traverse_front, cudaFuncAttributePreferredSharedMemoryCarveout, FLN_BH_CARVEOUT));
-  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_traverse, 32 * kWarps, 0));
-  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, bh_traverse_front, 32 * kWarps, 0));
+  const TraverseSet &TS = kTraverseSets[prm.bh_occupancy == 6 ? 1 : prm.bh_occupancy == 7 ? 2 : 0];
+  int per_sm = 64;
+  for (auto k : {TS.plain, TS.front, TS.cont}) {
+    FLN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, TS.carveout));
+    int n = 0;
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * kWarps, 0));
+    per_sm = std::min(per_sm, n);
+  }
   per_sm = std::max(per_sm, 1);
   const int grid = ctx.num_sms * per_sm;
-  const int grid_f = ctx.num_sms * std::max(std::min(per_sm_f, per_sm), 1);
+  const int grid_f = grid;
   const int64_t nwarps = (int64_t)grid * kWarps;
   const int spill_cap = prm.bh_spill_cap > 0 ? std::min(prm.bh_spill_cap, kSpill) : kSpill;
   int per_sm_l = 0;
@@ -2635,7 +2658,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         (front ? bh_traverse_learned_front : cont ? bh_traverse_learned_cont : bh_traverse_learned)
             <<<g, 32 * kWarps, 0, st>>>(A);
       else
-        (front ? bh_traverse_front : cont ? bh_traverse_cont : bh_traverse)<<<g, 32 * kWarps, 0, st>>>(A);
+        (front ? TS.front : cont ? TS.cont : TS.plain)<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
       BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc_exact, d_counts};
       FLN_CUDA(cudaEventRecord(ctx.ev_bk[0], st));

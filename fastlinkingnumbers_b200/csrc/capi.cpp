@@ -236,6 +236,8 @@ static fln_params resolved(const fln_params *p) {
     throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_retry_from_roots is 0 or 1");
   if (r.bh_spill_cap < 0 || r.bh_spill_cap > 8192) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_spill_cap in [0, 8192]");
   if (r.bh_wait_polls < 0) throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_wait_polls must not be negative");
+  if (r.bh_occupancy != 0 && (r.bh_occupancy < 5 || r.bh_occupancy > 7))
+    throw Error(FLN_ERR_INVALID_ARGUMENT, "bh_occupancy 0 or in [5, 7]");
   if (r.direct_tile < 0 || r.direct_tile >= kDirectTileShapes)
     throw Error(FLN_ERR_INVALID_ARGUMENT, "direct_tile in [0, " + std::to_string(kDirectTileShapes - 1) + "]");
   return r;
@@ -758,6 +760,7 @@ fln_status fln_autotune_direct(fln_ctx *ctx, const double *xyz, const int64_t *l
     r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
     r.best_beta = best.barnes_hut_init_beta;
     r.best_bucket = best.bh_bucket > 0 ? best.bh_bucket : 8;
+    r.best_occupancy = best.bh_occupancy > 0 ? best.bh_occupancy : 5;
     *out = best;
     if (result) *result = r;
   });
@@ -819,6 +822,19 @@ fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_off
     if (!t_beta && base.barnes_hut_init_beta != 1.5 && base.barnes_hut_init_beta != 2.0 &&
         base.barnes_hut_init_beta != 2.5 && base.barnes_hut_init_beta != 3.0)
       try_budgets(base);  // the caller's own beta
+    {  // traversal occupancy at the best setting (the same node pairs)
+      const fln_params around = best;
+      for (int occ : {6, 7}) {
+        fln_params p = around;
+        p.bh_occupancy = occ;
+        const double ms = time_of(p);
+        ++r.trials;
+        if (ms < r.best_ms) {
+          r.best_ms = ms;
+          best = p;
+        }
+      }
+    }
     if (t_bucket) {
       // Exact buckets of other sizes around the best setting so far (the
       // node pairs change: real sums move within the Barnes-Hut error).
@@ -837,6 +853,7 @@ fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_off
     r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
     r.best_beta = best.barnes_hut_init_beta;
     r.best_bucket = best.bh_bucket > 0 ? best.bh_bucket : 8;
+    r.best_occupancy = best.bh_occupancy > 0 ? best.bh_occupancy : 5;
     *out = best;
     if (result) *result = r;
   });

@@ -111,7 +111,9 @@ typedef struct fln_params {
                                    shared-memory tile): 0 = 128 x 256 (default), 1 = 128 x 128,
                                    2 = 128 x 512, 3 = 256 x 256, 4 = 256 x 512, 5 = 64 x 256; chosen by
                                    fln_autotune_direct. Sums change only in their rounding. */
-  int32_t reserved_i0;          /* zero */
+  int32_t bh_occupancy;         /* CTAs per SM of the Barnes-Hut traversal kernels: 0 = 5 (96 registers),
+                                   5, 6 (80 registers) or 7 (72, some spills); more resident warps hide more of
+                                   the traversal's dependent loads. Chosen by fln_autotune; results do not change */
   double reserved_params[4];    /* zero */
 } fln_params;
 
@@ -318,8 +320,9 @@ fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float 
  * on a seeded sample of the given pairs, `sample_pairs` of them (0 = 2048;
  * all pairs when there are fewer), for each traversal round budget
  * {128, 256, 512}; with bit 0 of tune_beta, also each initial beta
- * {1.5, 2, 2.5, 3}; with bit 1 (curve-order trees), then the exact-bucket
- * sizes {4, 6, 10, 12, 16} around the best setting. Beta and the bucket
+ * {1.5, 2, 2.5, 3}; then the traversal occupancies 6 and 7 CTAs per SM
+ * (fln_params.bh_occupancy) at the best setting; with bit 1 (curve-order
+ * trees), then the exact-bucket sizes {4, 6, 10, 12, 16} around it. Beta and the bucket
  * change the real sums within the Barnes-Hut error, never the certificate;
  * the budget changes only their rounding. *out gets *params with the
  * fastest setting; *result the sample times (device time, best of two runs
@@ -333,7 +336,7 @@ typedef struct fln_tune_result {
   int32_t best_direct_tile;  /* fln_autotune_direct */
   double best_beta;
   int32_t best_bucket;
-  int32_t reserved1;
+  int32_t best_occupancy;
   double reserved[2];
 } fln_tune_result;
 

@@ -304,7 +304,8 @@ def test_autotune_budget_keeps_results(engine):
     m = Model().SetCurves(3, -np.diff(off).astype(np.int32), xyz)
     poff, pxyz, pairs, _ = m.Prepare(True, engine=engine)
     tuned, res = engine.autotune(pxyz, poff, pairs, sample_pairs=64)
-    assert res["trials"] == 4 and res["sample_pairs"] == min(64, len(pairs))
+    assert res["trials"] == 6 and res["sample_pairs"] == min(64, len(pairs))
+    assert res["best_occupancy"] in (5, 6, 7)
     assert tuned.bh_budget in (128, 256, 512) and tuned.barnes_hut_init_beta == 2.0
     assert res["best_ms"] <= res["default_ms"]
     lk0, err0, fl0 = engine.linking_numbers(pxyz, poff, pairs, "barneshut")
@@ -312,12 +313,12 @@ def test_autotune_budget_keeps_results(engine):
     np.testing.assert_allclose(lk1, lk0, rtol=0, atol=1e-9)
     np.testing.assert_array_equal(fl1, fl0)
     tb, rb = engine.autotune(pxyz, poff, pairs, tune_beta=True, sample_pairs=64)
-    assert rb["trials"] == 13 and tb.barnes_hut_init_beta in (1.5, 2.0, 2.5, 3.0)
+    assert rb["trials"] == 15 and tb.barnes_hut_init_beta in (1.5, 2.0, 2.5, 3.0)
     lk2, _, _ = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tb)
     assert np.array_equal(np.rint(lk2), np.rint(lk0))
     # The exact-bucket size changes the node pairs, never the integers.
     tk, rk = engine.autotune(pxyz, poff, pairs, tune_bucket=True, sample_pairs=64)
-    assert rk["trials"] == 9 and rk["best_bucket"] in (4, 6, 8, 10, 12, 16)
+    assert rk["trials"] == 11 and rk["best_bucket"] in (4, 6, 8, 10, 12, 16)
     lk3, _, _ = engine.linking_numbers(pxyz, poff, pairs, "barneshut", params=tk)
     assert np.array_equal(np.rint(lk3), np.rint(lk0))
 
@@ -336,3 +337,20 @@ def test_direct_tile_shapes_and_autotune(engine, prec, tol, golden_dir):
     assert tuned.direct_tile == res["best_direct_tile"] and res["best_ms"] <= res["default_ms"]
     with pytest.raises(FlnError):
         engine.linking_numbers(xyz, off, pairs, "directsum", precision=prec, direct_tile=6)
+
+
+def test_traversal_occupancy_keeps_results(engine, golden_dir):
+    # The traversal kernels built for 5, 6 and 7 CTAs per SM walk the same node
+    # pairs; only the grouping of the FP64 partial sums differs (1e-9).
+    _, off, xyz, pairs = _prepared("knittubebroken", golden_dir)
+    lk5, err5, fl5 = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_occupancy=5)
+    s5 = engine.stats()
+    for occ in (6, 7):
+        lk, err, fl = engine.linking_numbers(xyz, off, pairs, "barneshut", bh_occupancy=occ)
+        s = engine.stats()
+        np.testing.assert_allclose(lk, lk5, rtol=0, atol=1e-9)
+        np.testing.assert_allclose(err, err5, rtol=1e-6, atol=1e-12)
+        np.testing.assert_array_equal(fl, fl5)
+        assert s["bh_far_evals"] == s5["bh_far_evals"] and s["bh_leaf_evals"] == s5["bh_leaf_evals"]
+    with pytest.raises(FlnError):
+        engine.linking_numbers(xyz, off, pairs, "barneshut", bh_occupancy=4)
