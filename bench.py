@@ -219,6 +219,8 @@ def run_ours(args, rank, world, local_rank):
     prm = N.default_params(precision=N.PREC_MIXED if args.precision == "mixed" else N.PREC_FP64,
                            bh_tree=args.bh_tree, bh_schedule=args.bh_schedule, bh_bucket=args.bh_bucket)
     tune = None
+    if args.bh_occupancy:
+        prm.bh_occupancy = args.bh_occupancy
     if args.bh_budget:
         prm.bh_budget = args.bh_budget
     elif args.autotune and args.method == "barneshut":
@@ -490,6 +492,9 @@ def main():
                     help="fixed Barnes-Hut round budget (skips the autotuner); 0 = tuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune the Barnes-Hut round budget on a sample of the pairs before timing")
+    ap.add_argument("--bh-occupancy", type=int, default=0,
+                    help="CTAs per SM of the traversal kernels (5, 6 or 7; 0 = the library's default or the "
+                         "autotuner's choice)")
     ap.add_argument("--autotune-bucket", type=int, default=1,
                     help="let the autotuner also choose the exact-bucket size (unless --bh-bucket is given)")
     ap.add_argument("--learned-leg", type=int, default=1,
