@@ -333,7 +333,7 @@ def run_ours(args, rank, world, local_rank):
                 "note": ("per step (all traversal rounds, CUDA events around each launch): algorithmic "
                          "bytes = 2 x 184 B FP32 node record per far-field node pair + 2 x 32 B (centre, "
                          "radius) per node pair handed to the exact list; traffic = DRAM read+write per "
-                         "node pair from the one-pass ncu capture in profiles/bh_traverse_polymer_10M_dram.md "
+                         "node pair from the one-pass ncu capture in profiles/launches_polymer_10M_bh.md "
                          "x node pairs; node records are mostly re-read from L1/L2: the kernel is bound by "
                          "L1 wavefronts and latency, not by HBM")}
     else:
@@ -348,7 +348,9 @@ def run_ours(args, rank, world, local_rank):
                          "tree": "curve-order" if args.bh_tree == 0 else "reference kd-median",
                          "schedule": ["rounds, fused evaluation", "persistent queue", "rounds, split evaluation"][args.bh_schedule],
                          "exact_bucket_segments": 1 if (args.bh_tree == 1 or args.bh_schedule != 0)
-                         else (args.bh_bucket or 8)},
+                         else (prm.bh_bucket or 8),
+                         "round_budget": prm.bh_budget or 256,
+                         "traversal_ctas_per_sm": prm.bh_occupancy or 5},
         "certificate_ms": ms,
         "autotune": tune,
         "e2e": {"value": world * units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
@@ -482,7 +484,7 @@ def main():
     ap.add_argument("--loop-steps", type=int, default=50000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-sample", type=int, default=64)
-    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=94.1,
+    ap.add_argument("--traffic-bytes-per-node-pair", type=float, default=66.4,
                     help="DRAM bytes per node pair measured by ncu on the polymer workload (0: none)")
     ap.add_argument("--cli-leg", type=int, default=1,
                     help="also time the verifycurves CLI end to end on the workload written as BCC")

@@ -37,6 +37,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <numeric>
 #include <type_traits>
@@ -61,7 +63,9 @@ constexpr int kWarps = 4;          // warps per traversal CTA
 #define FLN_BH_STACK 224
 #endif
 // Preferred shared-memory carveout of the traversal kernel, percent: room
-// for five CTAs of 15 KB (stacks, far-pair queue with its separations).
+// for five CTAs of up to 16 KB (stacks, far-pair queue with its separations,
+// and in the first pass the pairs' ratios for the frontier), 1 KB each
+// reserved by the system.
 #ifndef FLN_BH_CARVEOUT
 #define FLN_BH_CARVEOUT 44
 #endif
@@ -118,17 +122,18 @@ struct __align__(32) NodeHdr {
   int32_t right;
   int32_t lo;       // leaf: its segment; curve-order node: first segment of its range
   int32_t cnt;      // leaves below (curve-order: the range is [lo, lo + cnt))
-  int32_t pad[2];   // 64 B: two 32-byte loads (load_hdr), never across a 128 B line
-};
+  float tn;         // |c_M| and ||C_D||_F / sqrt(3) of the node's moments: the
+  float dn;         // Eq. 14 weights, formed when a pair is classified far
+};                  // 64 B: two 32-byte loads (load_hdr), never across a 128 B line
 static_assert(sizeof(NodeHdr) == 64, "NodeHdr layout");
 struct __align__(32) NodeMom {
   float t[3];
   float D[9];
   float Q[18];
-  float tn, dn, qn;
-  float pad[7];     // 160 B: five 32-byte loads (load_mom)
+  float qn;         // (1/3) ||C_Q||_F
+  float pad;        // 128 B: four 32-byte loads (load_mom), one 128 B line
 };
-static_assert(sizeof(NodeMom) == 160, "NodeMom layout");
+static_assert(sizeof(NodeMom) == 128, "NodeMom layout");
 
 // Traversal records through the read-only path in 32-byte loads: the
 // traversal is bound by L1 wavefronts, and a scattered 32-byte load costs
@@ -149,7 +154,7 @@ __device__ __forceinline__ NodeMom load_mom(const NodeMom *p) {
   NodeMom m;
   unsigned long long *w = reinterpret_cast<unsigned long long *>(&m);
 #pragma unroll
-  for (int i = 0; i < 5; ++i) load32(reinterpret_cast<const char *>(p) + 32 * i, w + 4 * i);
+  for (int i = 0; i < 4; ++i) load32(reinterpret_cast<const char *>(p) + 32 * i, w + 4 * i);
   return m;
 }
 
@@ -300,7 +305,6 @@ __device__ void finish_record_regs(const BuildNode &B, NodeHdr &H, NodeMom &M, b
   H.right = leaf ? -1 : r;
   H.lo = B.seg_lo;
   H.cnt = B.seg_cnt;
-  H.pad[0] = H.pad[1] = 0;
   const double tn = sqrt(B.t[0] * B.t[0] + B.t[1] * B.t[1] + B.t[2] * B.t[2]);
   double dd = 0, qq = 0;
   for (int a = 0; a < 9; ++a) dd += B.D[a] * B.D[a];
@@ -309,11 +313,11 @@ __device__ void finish_record_regs(const BuildNode &B, NodeHdr &H, NodeMom &M, b
   for (int a = 0; a < 3; ++a) M.t[a] = (float)B.t[a];
   for (int a = 0; a < 9; ++a) M.D[a] = (float)B.D[a];
   for (int a = 0; a < 18; ++a) M.Q[a] = (float)B.Q[a];
-  M.tn = (float)tn;
-  M.dn = (float)(sqrt(dd) * kInvRt3);
+  H.tn = (float)tn;
+  H.dn = (float)(sqrt(dd) * kInvRt3);
   // Leaf: |c|^3 / 36, which is also (1/3) ||C_Q||_F for c c c^T / 12.
   M.qn = (float)(leaf ? tn * tn * tn / 36.0 : sqrt(qq) / 3.0);
-  for (int a = 0; a < 7; ++a) M.pad[a] = 0.f;
+  M.pad = 0.f;
 }
 
 // Traversal records of a node, formed in registers and stored as vectors.
@@ -533,13 +537,28 @@ struct Batch {
 
 // Frontier of a Barnes–Hut pass: the far node pairs of one loop pair (slot),
 // up to kFrontPairs per record, recorded so that the beta retry can continue
-// from them instead of from the roots.
+// from them instead of from the roots. Beside each pair, its separation
+// ratio (|dr|^2 + eps^2 - eps^2) / (r1 + r2)^2 in FP32 (front_ratio): a pair
+// whose ratio clears the retry's beta^2 by a margin far above the FP32
+// rounding is far at that beta without loading its headers.
 constexpr int kFrontPairs = 128;
 struct FrontRec {
   int32_t slot;
   int32_t count;
   int2 pairs[kFrontPairs];
+  float ratio[kFrontPairs];
 };
+// The ratio in FP32 from the FP64 quantities of the far test: three roundings
+// (two conversions, one __fdividef of at most 2 ulp), so it lies within
+// 4e-7 of the FP64 ratio. 0 (never clear) when (r1 + r2)^2 is below 1e-30,
+// where the FP32 quotient is not trusted.
+__device__ __forceinline__ float front_ratio(double dsq, double eps, double rs) {
+  const double den = rs * rs;
+  return den >= 1e-30 ? __fdividef((float)(dsq - eps), (float)den) : 0.f;
+}
+// A frontier pair is left to the full test unless ratio > beta^2 (1 + 1e-5):
+// then |dr|^2 + eps^2 > (r1 + r2)^2 beta^2 + eps^2 holds in FP64 as well.
+__device__ __forceinline__ float front_clear(double itolsq) { return (float)(itolsq * (1.0 + 1e-5)); }
 
 struct TravArgs {
   const double *xyz;
@@ -616,11 +635,21 @@ __device__ __forceinline__ float qrow(const float *q, int i, float rx, float ry,
 #ifndef FLN_FAR_FP32_SCALE
 #define FLN_FAR_FP32_SCALE 1
 #endif
+// The Eq. 14 weights of a node pair (compute_link.cpp:411-524), from the
+// headers the classification loaded: the moment records of a far pair are
+// then read once, at evaluation, and fill one 128-byte line each.
+__device__ __forceinline__ float2 far_weights(const NodeHdr &h1, const NodeHdr &h2) {
+  const float r1 = (float)h1.r, r2 = (float)h2.r;
+  return make_float2(__fmaf_rn(r1, h2.tn, __fmul_rn(3.f, h2.dn)), __fmaf_rn(r2, h1.tn, __fmul_rn(3.f, h1.dn)));
+}
+
 // Far-field pair: monopole + Eq. 29 + Eq. 30 times 1/(4 pi |r|^3), and the
 // Eq. 14 estimate with the same factor (compute_link.cpp:608-627, :411-524).
 // Node 1 = u (moments m1 = "C" in the reference), node 2 = v ("D").
-__device__ void far_eval(const NodeMom &m1, const NodeMom &m2, float rx, float ry, float rz, double dsq, float r1,
-                         float r2, double &sum, double &err) {
+// ea1 = r_u |c_v| + 3 ||C_D,v|| / sqrt(3) and ea2 the same with u and v
+// swapped (far_weights, from the two headers) weight the quadrupole norms.
+__device__ void far_eval(const NodeMom &m1, const NodeMom &m2, float rx, float ry, float rz, double dsq, float ea1,
+                         float ea2, double &sum, double &err) {
   const float *C3 = m1.D, *D3 = m2.D;
   const float C1x = m1.t[0], C1y = m1.t[1], C1z = m1.t[2];
   const float D1x = m2.t[0], D1y = m2.t[1], D1z = m2.t[2];
@@ -699,7 +728,6 @@ __device__ void far_eval(const NodeMom &m1, const NodeMom &m2, float rx, float r
   const double mult = 1.0 / (dsq * sqrt(dsq)) * kInvFourPi;
 #endif
   sum += mult * ((double)res + (double)ho);
-  const float ea1 = __fmaf_rn(r1, m2.tn, __fmul_rn(3.f, m2.dn)), ea2 = __fmaf_rn(r2, m1.tn, __fmul_rn(3.f, m1.dn));
   const float e = __fmul_rn(rdist2, __fmaf_rn(m1.qn, ea1, __fmul_rn(m2.qn, ea2)));
   err = __fma_rn(mult, (double)e, err);
 }
@@ -798,7 +826,7 @@ __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefe
 template <class T>
 __device__ __forceinline__ void prefetch_record(const T *p) {
   prefetch_l1(p);
-  prefetch_l1(reinterpret_cast<const char *>(p) + sizeof(T) - 1);
+  if constexpr (sizeof(T) > 128) prefetch_l1(reinterpret_cast<const char *>(p) + sizeof(T) - 1);
 }
 
 // stack[0, n) = stack[k, k + n), warp-wide, in passes of 32 that read before
@@ -817,12 +845,13 @@ __device__ __noinline__ void shift_down(int2 *stack, int k, int n, int lane) {
   }
 }
 
-// Appends n (<= 32) far node pairs, one per lane (lanes < n), to the warp's
+// Appends n (<= 32) far node pairs and their separation ratios (front_ratio),
+// one per lane (lanes < n), to the warp's
 // open frontier record of `slot`, reserving records as they fill. The open
 // record is (fr, ffill); fr < 0 means none. A record is closed (its header
 // written) when it is full, when the warp moves to another slot, or when the
 // warp finishes.
-__device__ __forceinline__ void front_close(const TravArgs &A, long long &fr, int &ffill, int slot, int lane) {
+__device__ __forceinline__ void front_close(const TravArgs &A, int &fr, int &ffill, int slot, int lane) {
   if (fr >= 0 && lane == 0 && fr < A.front_cap) {
     A.front[fr].slot = slot;
     A.front[fr].count = ffill;
@@ -830,19 +859,24 @@ __device__ __forceinline__ void front_close(const TravArgs &A, long long &fr, in
   fr = -1;
   ffill = 0;
 }
-__device__ __forceinline__ void front_put(const TravArgs &A, long long &fr, int &ffill, int slot, int2 q, int n,
-                                          int lane) {
+__device__ __forceinline__ void front_put(const TravArgs &A, int &fr, int &ffill, int slot, int2 q, float ratio,
+                                          int n, int lane) {
   const int need = (fr < 0 ? 1 : 0) + (ffill + n > kFrontPairs ? 1 : 0);
-  long long c = 0;
-  if (lane == 0 && need) c = (long long)atomicAdd(A.front_count, (unsigned long long)need);
+  int c = 0;  // record index (clamped: past the capacity only "lost" matters)
+  if (lane == 0 && need)
+    c = (int)min(atomicAdd(A.front_count, (unsigned long long)need), (unsigned long long)(INT_MAX - 1));
   c = __shfl_sync(0xffffffffu, c, 0);
-  const long long cur = fr < 0 ? c : fr, nxt = fr < 0 ? c + 1 : c;
+  const int cur = fr < 0 ? c : fr, nxt = fr < 0 ? c + 1 : c;
   const int pos = ffill + lane;
-  const long long dst = pos < kFrontPairs ? cur : nxt;
-  if (lane < n && dst < A.front_cap) A.front[dst].pairs[pos < kFrontPairs ? pos : pos - kFrontPairs] = q;
+  const int dst = pos < kFrontPairs ? cur : nxt;
+  if (lane < n && dst < A.front_cap) {
+    const int at = pos < kFrontPairs ? pos : pos - kFrontPairs;
+    A.front[dst].pairs[at] = q;
+    A.front[dst].ratio[at] = ratio;
+  }
   if (lane == 0 && (cur >= A.front_cap || (ffill + n > kFrontPairs && nxt >= A.front_cap))) A.front_lost[slot] = 1;
   if (ffill + n >= kFrontPairs) {
-    long long full = cur;
+    int full = cur;
     int nfull = kFrontPairs;
     front_close(A, full, nfull, slot, lane);
     fr = ffill + n > kFrontPairs ? nxt : -1;
@@ -866,20 +900,28 @@ __device__ __forceinline__ void front_put(const TravArgs &A, long long &fr, int 
 //
 // The continued retry (kMode 2) keeps the first pass's far-field and error
 // sums of the slot. A node pair's far-field value and estimate do not depend
-// on beta, so a frontier pair (marked by bit 31 of its first node id) that is
-// still far at the slot's beta is left alone: its value is already in the
-// sums. A frontier pair that is opened now has its first-pass value and
+// on beta, so a frontier pair that is still far at the slot's beta is left
+// alone: its value is already in the sums. Most such pairs are recognised at
+// intake from the ratio recorded with them (front_clear); the rest go on the
+// stack marked by bit 31 of their first node id and take the full test. A frontier pair that is opened now has its first-pass value and
 // estimate subtracted (queued with a negative squared separation, evaluated
 // at the one far-field call site, so the value is the one the first pass
 // added) and is then exact or split like any pair.
 constexpr int kFrontFlag = int(0x80000000u);
+// Sum of a per-lane 32-bit count over the warp, in FP64 (no overflow).
+__device__ __forceinline__ double warp_sum_u32(unsigned v) {
+  unsigned long long s = v;
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return (double)s;
+}
 template <bool kLearn, bool kRecord, int kMode>
 __device__ __forceinline__ void traverse(const TravArgs &A) {
   constexpr bool kFront = kMode == 1, kCont = kMode == 2;
   __shared__ int2 s_stack[kWarps][kStack];
   __shared__ int2 s_far[kWarps][64];
   __shared__ float4 s_farv[kWarps][64];  // separation (x, y, z) and its square (negative: subtract), per queued far pair
-  __shared__ float2 s_farr[kWarps][64];  // the two radii
+  __shared__ float2 s_farr[kWarps][64];  // the two Eq. 14 weights (far_weights)
+  __shared__ float s_fart[kWarps][kFront ? 64 : 1];  // separation ratios for the frontier (front_ratio)
   __shared__ std::conditional_t<kLearn, MlpFrag, int> s_mlp;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + w;
@@ -887,6 +929,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   int2 *farq = s_far[w];
   float4 *farv = s_farv[w];
   float2 *farr = s_farr[w];
+  float *fart = s_fart[w];
   if constexpr (kLearn) {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(A.learned.frag);
     uint32_t *dst = reinterpret_cast<uint32_t *>(&s_mlp);
@@ -894,8 +937,10 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     __syncthreads();
   }
   int2 *spill = A.spill + (size_t)gw * kSpill;
-  double nfar = 0, nent = 0, nreuse = 0, nsub = 0;
-  long long frec = -1;  // open frontier record (kFront)
+  // Per-lane counts in 32 bits (a lane classifies at most one node pair per
+  // step, and a launch's steps are bounded by its batches' budgets).
+  unsigned nfar = 0, nent = 0, nreuse = 0, nsub = 0;
+  int frec = -1;  // open frontier record (kFront)
   int ffill = 0, fslot = -1;
   const long long total = A.nin + A.nin1;
   for (;;) {
@@ -932,13 +977,33 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     const double itolsq = A.itolsq[slot], eps = A.epssq;
     // Threshold of the learned criterion: tau x (beta0 / beta)^4 in later passes.
     const float log10_tau = A.learned.log10_tau + 2.f * (float)log10(A.beta0 * A.beta0 / itolsq);
-    for (int x = lane; x < cnt0; x += 32) {
-      int2 v = src[x];
-      if (kCont && from_front) v.x |= kFrontFlag;
-      stack[x] = v;
+    int top = cnt0;
+    if (kCont && from_front) {
+      // Frontier pairs still clearly far at this slot's beta keep their
+      // first-pass value and need no classification; the others go on the
+      // stack, marked, for the full test.
+      const float clear = front_clear(itolsq);
+      const float *ratio = A.in1[b - A.nin].ratio;
+      top = 0;
+      for (int x0 = 0; x0 < cnt0; x0 += 32) {
+        const int x = x0 + lane;
+        int2 v = make_int2(0, 0);
+        bool keep = false;
+        if (x < cnt0) {
+          v = src[x];
+          keep = !(ratio[x] > clear);
+          nreuse += keep ? 0u : 1u;
+        }
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        v.x |= kFrontFlag;
+        if (keep) stack[top + __popc(km & ((1u << lane) - 1))] = v;
+        top += __popc(km);
+      }
+    } else {
+      for (int x = lane; x < cnt0; x += 32) stack[x] = src[x];
     }
-    int top = cnt0, nspill = 0, nf = 0, steps = 0;
-    long long bc = -1;  // open chunk of the exact list
+    int nspill = 0, nf = 0, steps = 0;
+    int bc = -1;  // open chunk of the exact list
     int bfill = 0;      // entries in it
     bool overflow = false;
     double sum = 0.0, err = 0.0;
@@ -1002,6 +1067,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         double dsq = 0.0;
         float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 fr = make_float2(0.f, 0.f);
+        float fratio = 0.f;  // separation ratio for the frontier (kFront)
         int mincnt = 0;  // segments of the smaller node (learned criterion)
         if (act) {
           const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
@@ -1010,7 +1076,8 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
           const double rs = h1.r + h2.r;
           dsq = dx * dx + dy * dy + dz * dz + eps;
           fv = make_float4((float)dx, (float)dy, (float)dz, (float)dsq);
-          fr = make_float2((float)h1.r, (float)h2.r);
+          fr = far_weights(h1, h2);
+          if constexpr (kFront) fratio = front_ratio(dsq, eps, rs);
           sep = (float)(sqrt(dsq) / rs);
           if constexpr (kLearn) mincnt = min(h1.cnt, h2.cnt);
           if (leaf1 && leaf2) {
@@ -1056,8 +1123,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
             for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
             if (cand) {
               const NodeHdr h1 = load_hdr(H1 + pr.x), h2 = load_hdr(H2 + pr.y);
-              const NodeMom &ma = M1[pr.x], &mb = M2[pr.y];
-              mlp_features(sep, (float)h1.r, (float)h2.r, dsq, ma.tn, mb.tn, ma.dn, mb.dn, ma.qn, mb.qn, f);
+              mlp_features(sep, (float)h1.r, (float)h2.r, dsq, h1.tn, h2.tn, h1.dn, h2.dn, M1[pr.x].qn, M2[pr.y].qn, f);
             }
             const float y = mlp_warp_predict(reinterpret_cast<const MlpFrag &>(s_mlp), f);
             if (cand && y < log10_tau) kind = 2;
@@ -1108,6 +1174,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
             farq[at] = pr;
             farv[at] = fv;
             farr[at] = fr;
+            if constexpr (kFront) fart[at] = fratio;
           }
 #if FLN_BH_PREFETCH & 2
           if (kind == 2 || sub) {
@@ -1120,11 +1187,12 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
             const int ne = __popc(lm), pos = bfill + __popc(lm & ((1u << lane) - 1));
             nent += ne;
             const int need = (bc < 0 ? 1 : 0) + (bfill + ne > 32 ? 1 : 0);
-            long long c = 0;
-            if (lane == 0 && need) c = (long long)atomicAdd(A.bkt_count, (unsigned long long)need);
+            int c = 0;  // chunk index (clamped: past the capacity the status flags it)
+            if (lane == 0 && need)
+              c = (int)min(atomicAdd(A.bkt_count, (unsigned long long)need), (unsigned long long)(INT_MAX - 1));
             c = __shfl_sync(0xffffffffu, c, 0);
-            const long long cur = bc < 0 ? c : bc, nxt = bc < 0 ? c + 1 : c;
-            const long long dst = pos < 32 ? cur : nxt;
+            const int cur = bc < 0 ? c : bc, nxt = bc < 0 ? c + 1 : c;
+            const int dst = pos < 32 ? cur : nxt;
             if (kind == 1) {
               if (dst < A.bkt_cap) A.bkt[dst].e[pos & 31] = ex;
               else atomicOr(A.status, 4);
@@ -1151,10 +1219,10 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         const int m = min(nf, 32);
         int2 q = make_int2(0, 0);
         if (lane < m) q = farq[nf - m + lane];
-        if constexpr (kFront) front_put(A, frec, ffill, slot, q, m, lane);
+        if constexpr (kFront) front_put(A, frec, ffill, slot, q, lane < m ? fart[nf - m + lane] : 0.f, m, lane);
         if (lane < m) {
           const float4 v = farv[nf - m + lane];
-          const float2 rr = farr[nf - m + lane];
+          const float2 rr = farr[nf - m + lane];  // Eq. 14 weights
           double fs = 0.0, fe = 0.0;
           far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)fabsf(v.w), rr.x, rr.y, fs, fe);
           if (v.w < 0.f) {
@@ -1185,19 +1253,16 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     }
   }
   if constexpr (kFront) front_close(A, frec, ffill, fslot, lane);
-  for (int o = 16; o; o >>= 1) {
-    nfar += __shfl_xor_sync(0xffffffffu, nfar, o);
-    if constexpr (kCont) {
-      nreuse += __shfl_xor_sync(0xffffffffu, nreuse, o);
-      nsub += __shfl_xor_sync(0xffffffffu, nsub, o);
-    }
-  }
+  const double wfar = warp_sum_u32(nfar);
   if (lane == 0) {
-    atomicAdd(A.counts, nfar);
-    atomicAdd(A.counts + 5, nent);
-    if constexpr (kCont) {
-      atomicAdd(A.counts + 6, nreuse);
-      atomicAdd(A.counts + 7, nsub);
+    atomicAdd(A.counts, wfar);
+    atomicAdd(A.counts + 5, (double)nent);
+  }
+  if constexpr (kCont) {
+    const double wreuse = warp_sum_u32(nreuse), wsub = warp_sum_u32(nsub);
+    if (lane == 0) {
+      atomicAdd(A.counts + 6, wreuse);
+      atomicAdd(A.counts + 7, wsub);
     }
   }
 }
@@ -1232,11 +1297,16 @@ struct BucketArgs {
 constexpr int kBkWarps = 4;     // warps per CTA
 constexpr int kStageV = 320;    // staged loop-2 vertices per warp (32 entries of up to 9, or 16 of up to 17)
 
+// Near steps as a select rather than a branch (1) or a branch (0).
+#ifndef FLN_BK_NEAR_SELECT
+#define FLN_BK_NEAR_SELECT 0
+#endif
 struct SegWalkF {        // the carried state of a walk along loop 2 (FP32)
   float ax, ay, az;      // a = q_k - p0
   float bx, by, bz;      // b = q_k - p1
   float aa, bb, ab;      // |a|^2, |b|^2, a.b
   float la, lb;          // |a|, |b|
+  float mn;              // min(|a|^2, |b|^2)
 };
 
 __device__ __forceinline__ SegWalkF walk_start_f(float p0x, float p0y, float p0z, float4 q0, float ex, float ey,
@@ -1253,26 +1323,36 @@ __device__ __forceinline__ SegWalkF walk_start_f(float p0x, float p0y, float p0z
   w.ab = dot3(w.ax, w.ay, w.az, w.bx, w.by, w.bz);
   w.la = norm_of(w.aa);
   w.lb = norm_of(w.bb);
+  w.mn = fminf(w.aa, w.bb);
   return w;
 }
 
 // One step q0 -> q1 of the walk (q1.w unused; ff = |q1 - q0|^2 comes from
-// the staged vertex q0), from FP32 coordinates relative to an origin. The
+// the staged vertex q0), from FP32 coordinates relative to an origin: reads
+// the state w at q0 and writes the state o at q1 (a walk alternates two
+// states, so that no step copies one). The
 // arctangent: when div1 + div2 > 0 and |y| < x / 4 the principal branch by
 // the 5-term series (|angle| < 0.245), otherwise atan2f and the branch turn
 // of the reference (compute_link.cpp:151-175). (A branch-free arctangent,
 // range reduced by pi/6, measured slower on B200: the slow path is rare
 // enough that the warps seldom diverge on it.)
-__device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, float p0z, float4 q1, float ff,
-                                            float ex, float ey, float ez, float ee, float &acc, float &turns) {
+__device__ __forceinline__ bool walk_step_f(const SegWalkF &w, SegWalkF &o, float p0x, float p0y, float p0z, float4 q1,
+                                            float ff, float ex, float ey, float ez, float ee, float &acc, float &turns) {
   const float dx = q1.x - p0x, dy = q1.y - p0y, dz = q1.z - p0z;
   const float fx = dx - w.ax, fy = dy - w.ay, fz = dz - w.az;
   const float cx = dx - ex, cy = dy - ey, cz = dz - ez;
   const float cc = dot3(cx, cy, cz, cx, cy, cz), dd = dot3(dx, dy, dz, dx, dy, dz);
   const float cd = dot3(cx, cy, cz, dx, dy, dz);
   const float lc = norm_of(cc), ld = norm_of(dd);
-  const bool near = fminf(fminf(w.aa, w.bb), fminf(cc, dd)) <= fmaxf(ee, ff);
+  const float mn = fminf(cc, dd);
+  const bool near = fminf(w.mn, mn) <= fmaxf(ee, ff);
+#if FLN_BK_NEAR_SELECT
+  // Every step forms the term; a near step (left to FP64) drops it by a
+  // select, so only the rare slow arctangent is a branch.
+  {
+#else
   if (!near) {
+#endif
     const float ca = dot3(cx, cy, cz, w.ax, w.ay, w.az), cb = dot3(cx, cy, cz, w.bx, w.by, w.bz);
     const float ad = dot3(w.ax, w.ay, w.az, dx, dy, dz);
     const float det = w.ax * (fy * ez - fz * ey) + w.ay * (fz * ex - fx * ez) + w.az * (fx * ey - fy * ex);
@@ -1280,22 +1360,41 @@ __device__ __forceinline__ bool walk_step_f(SegWalkF &w, float p0x, float p0y, f
     const float div1 = t * w.lb + w.ab * lc + ca * w.lb + cb * w.la;
     const float div2 = t * ld + ad * lc + ca * ld + cd * w.la;
     const float x = div1 * div2 - det * det;
-    const float s = (det == 0.f) ? copysignf(1.f, div1) + copysignf(1.f, div2) : (div1 + div2);
-    const float y = det * s;
+    // s = div1 + div2 serves the fast path also when det = 0: y is then a
+    // zero of det's sign under both forms of s, and the test below holds
+    // under both exactly when div1 > 0 and div2 > 0. The other branch forms
+    // the reference's s (compute_link.cpp:151-175).
+    float s = div1 + div2;
+    float y = det * s;
+#if FLN_BK_NEAR_SELECT
+    const bool fast = s > 0.f && fabsf(y) < 0.25f * x;
+    float term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
+    if (!fast && !near) {
+#else
     float term;
     if (s > 0.f && fabsf(y) < 0.25f * x) {
       term = atan_quarter(__fdividef(y, x));  // principal branch, |angle| < 0.245
     } else {
+#endif
+      if (det == 0.f) {
+        s = copysignf(1.f, div1) + copysignf(1.f, div2);
+        y = det * s;
+      }
       term = atan2f(y, x);
       const float sg = (det == 0.f) ? -copysignf(1.f, div1) : copysignf(1.f, det);
       if ((s < 0.f) || ((s == 0.f) && (det < 0.f))) turns += sg;
     }
+#if FLN_BK_NEAR_SELECT
+    acc += near ? 0.f : term;
+#else
     acc += term;
+#endif
   }
-  w.ax = dx; w.ay = dy; w.az = dz;
-  w.bx = cx; w.by = cy; w.bz = cz;
-  w.aa = dd; w.bb = cc; w.ab = cd;
-  w.la = ld; w.lb = lc;
+  o.ax = dx; o.ay = dy; o.az = dz;
+  o.bx = cx; o.by = cy; o.bz = cz;
+  o.aa = dd; o.bb = cc; o.ab = cd;
+  o.la = ld; o.lb = lc;
+  o.mn = mn;
   return !near;
 }
 
@@ -1322,9 +1421,10 @@ __device__ __forceinline__ double seg_pair_term(const double *xyz, int64_t o1, i
   const float p0x = (float)(p0[0] - ox), p0y = (float)(p0[1] - oy), p0z = (float)(p0[2] - oz);
   const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
   const float ee = dot3(ex, ey, ez, ex, ey, ez);
-  SegWalkF w = walk_start_f(p0x, p0y, p0z, f0, ex, ey, ez);
+  const SegWalkF w = walk_start_f(p0x, p0y, p0z, f0, ex, ey, ez);
+  SegWalkF o;
   float acc = 0.f, turns = 0.f;
-  if (walk_step_f(w, p0x, p0y, p0z, f1, f0.w, ex, ey, ez, ee, acc, turns))
+  if (walk_step_f(w, o, p0x, p0y, p0z, f1, f0.w, ex, ey, ez, ee, acc, turns))
     return kInvTwoPi * (double)acc + (double)turns;
   return seg_term_fp64(xyz, a0, a1, b0, b1);
 }
@@ -1436,8 +1536,6 @@ __global__ void __launch_bounds__(32 * kBkWarps, FLN_BUCKET_MIN_CTAS) bh_buckets
         const int lo1 = __shfl_sync(0xffffffffu, e.x, j), lo2 = __shfl_sync(0xffffffffu, e.y, j);
         const int c2 = __shfl_sync(0xffffffffu, e.w, j), vbj = __shfl_sync(0xffffffffu, vb, j);
         const bool act = g < nrows;
-        // The warp walks as far as its longest row (rows are sorted).
-        const int wmax = __reduce_max_sync(0xffffffffu, act ? c2 : 0);
         uint32_t nearmask = 0;  // steps of this lane's row left to FP64
         int s1 = 0;
         if (act) {
@@ -1451,15 +1549,21 @@ __global__ void __launch_bounds__(32 * kBkWarps, FLN_BUCKET_MIN_CTAS) bh_buckets
           const float p0x = (float)(p0[0] - ox), p0y = (float)(p0[1] - oy), p0z = (float)(p0[2] - oz);
           const float ex = (float)(p1[0] - p0[0]), ey = (float)(p1[1] - p0[1]), ez = (float)(p1[2] - p0[2]);
           const float ee = dot3(ex, ey, ez, ex, ey, ez);
-          float4 q0 = sq[vbj];
-          SegWalkF w = walk_start_f(p0x, p0y, p0z, q0, ex, ey, ez);
-          float acc = 0.f, turns = 0.f;
-          for (int k = 0; k < wmax; ++k) {
-            if (k < c2) {
-              const float4 q1 = sq[vbj + k + 1];
-              if (!walk_step_f(w, p0x, p0y, p0z, q1, q0.w, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
-              q0 = q1;
-            }
+          const float4 q0 = sq[vbj];
+          SegWalkF wa = walk_start_f(p0x, p0y, p0z, q0, ex, ey, ez), wb;
+          float ff = q0.w, acc = 0.f, turns = 0.f;
+          // Two steps per pass, the state going wa -> wb -> wa. Rows are
+          // sorted, so the lanes of a warp mostly walk equally far.
+          int k = 0;
+          for (; k + 2 <= c2; k += 2) {
+            const float4 q1 = sq[vbj + k + 1], q2 = sq[vbj + k + 2];
+            if (!walk_step_f(wa, wb, p0x, p0y, p0z, q1, ff, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
+            if (!walk_step_f(wb, wa, p0x, p0y, p0z, q2, q1.w, ex, ey, ez, ee, acc, turns)) nearmask |= 2u << k;
+            ff = q2.w;
+          }
+          if (k < c2) {
+            const float4 q1 = sq[vbj + k + 1];
+            if (!walk_step_f(wa, wb, p0x, p0y, p0z, q1, ff, ex, ey, ez, ee, acc, turns)) nearmask |= 1u << k;
           }
           sum += kInvTwoPi * (double)acc + (double)turns;
         }
@@ -1522,10 +1626,10 @@ FLN_TRAVERSE_KERNELS(7)
 struct TraverseSet {
   void (*plain)(TravArgs), (*front)(TravArgs), (*cont)(TravArgs);
   int ctas;       // CTAs per SM the set is built for
-  int carveout;   // shared-memory carveout (percent) that fits that many CTAs of 15 KB
+  int carveout;   // shared-memory carveout (percent) that fits that many CTAs of 16 KB
 };
 const TraverseSet kTraverseSets[] = {{bh_traverse_o5, bh_traverse_front_o5, bh_traverse_cont_o5, 5, FLN_BH_CARVEOUT},
-                                     {bh_traverse_o6, bh_traverse_front_o6, bh_traverse_cont_o6, 6, FLN_BH_CARVEOUT},
+                                     {bh_traverse_o6, bh_traverse_front_o6, bh_traverse_cont_o6, 6, 58},
                                      {bh_traverse_o7, bh_traverse_front_o7, bh_traverse_cont_o7, 7, 58}};
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, 0>(A); }
 // The learned kernels at FLN_LEARNED_MIN_CTAS CTAs per SM: their MLP code
@@ -1763,8 +1867,9 @@ __global__ void __launch_bounds__(256) bh_far_chunks(EvalArgs A) {
     const int2 q = A.chunks[c].pairs[lane];
     const NodeHdr h1 = load_hdr(A.hdr + b1 + q.x), h2 = load_hdr(A.hdr + b2 + q.y);
     const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+    const float2 w = far_weights(h1, h2);
     far_eval(load_mom(A.mom + b1 + q.x), load_mom(A.mom + b2 + q.y), (float)dx, (float)dy, (float)dz,
-             dx * dx + dy * dy + dz * dz + A.epssq, (float)h1.r, (float)h2.r, sum, err);
+             dx * dx + dy * dy + dz * dz + A.epssq, w.x, w.y, sum, err);
   }
   for (int o = 16; o; o >>= 1) {
     sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -2152,8 +2257,9 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
         const int2 q = farq[nf - 32 + lane];
         const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
         const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
+        const float2 w = far_weights(h1, h2);
         far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps,
-                 (float)h1.r, (float)h2.r, sum, err);
+                 w.x, w.y, sum, err);
         nfar += 32;
         nf -= 32;
         __syncwarp();
@@ -2170,8 +2276,9 @@ __global__ void __launch_bounds__(32 * kWarps) bh_persistent(PersistArgs A) {
       const int2 q = farq[lane];
       const NodeHdr h1 = load_hdr(H1 + q.x), h2 = load_hdr(H2 + q.y);
       const double dx = h2.m[0] - h1.m[0], dy = h2.m[1] - h1.m[1], dz = h2.m[2] - h1.m[2];
-      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, (float)h1.r,
-               (float)h2.r, sum, err);
+      const float2 w = far_weights(h1, h2);
+      far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), (float)dx, (float)dy, (float)dz, dx * dx + dy * dy + dz * dz + eps, w.x,
+               w.y, sum, err);
     }
     if (lane < nl) {
       const int2 q = leafq[lane];
@@ -2221,10 +2328,11 @@ __global__ void sample_features(const int64_t *node_base, const NodeHdr *hdr, co
   const double dsq = dx * dx + dy * dy + dz * dz + epssq;
   const float sep = (float)(sqrt(dsq) / (h1.r + h2.r));
   float f[kMlpIn];
-  mlp_features(sep, (float)h1.r, (float)h2.r, dsq, m1.tn, m2.tn, m1.dn, m2.dn, m1.qn, m2.qn, f);
+  mlp_features(sep, (float)h1.r, (float)h2.r, dsq, h1.tn, h2.tn, h1.dn, h2.dn, m1.qn, m2.qn, f);
   for (int i = 0; i < kMlpIn; ++i) X[k * kMlpIn + i] = f[i];
   double v = 0.0, e = 0.0;
-  far_eval(m1, m2, (float)dx, (float)dy, (float)dz, dsq, (float)h1.r, (float)h2.r, v, e);
+  const float2 w = far_weights(h1, h2);
+  far_eval(m1, m2, (float)dx, (float)dy, (float)dz, dsq, w.x, w.y, v, e);
   approx[k] = v;
   sep_out[k] = sep;
   est_out[k] = (float)log10(e * err_scale + 1e-30);
@@ -2506,6 +2614,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   // [0] queue, [1] next-round count, [2] exact (or far) chunks, [3] leaf chunks, [4] frontier records
   unsigned long long *d_ctr = d_acc + 3 * np;
   const TraverseSet &TS = kTraverseSets[prm.bh_occupancy == 6 ? 1 : prm.bh_occupancy == 7 ? 2 : 0];
+  static const bool round_log = std::getenv("FLN_BH_ROUND_LOG") != nullptr;
   int per_sm = 64;
   for (auto k : {TS.plain, TS.front, TS.cont}) {
     FLN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, TS.carveout));
@@ -2671,6 +2780,14 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       FLN_CUDA(cudaMemcpyAsync(c2, d_ctr, sizeof c2, cudaMemcpyDeviceToHost, st));
       FLN_CUDA(cudaStreamSynchronize(st));
       ctx.stats.ms_exact += ctx.elapsed(ctx.ev_bk[0], ctx.ev_bk[1]);
+      if (round_log) {  // FLN_BH_ROUND_LOG: cumulative counts after each round, for profiling
+        double cnt[8];
+        FLN_CUDA(cudaMemcpyAsync(cnt, d_counts, sizeof cnt, cudaMemcpyDeviceToHost, st));
+        FLN_CUDA(cudaStreamSynchronize(st));
+        std::fprintf(stderr, "[fln] round %d (%s): far node pairs %.0f, exact node pairs %.0f, exact segment pairs %.0f\n",
+                     ctx.stats.bh_rounds, front ? "first pass" : cont ? "continued retry" : "from roots", cnt[0],
+                     cnt[5], cnt[1]);
+      }
       // Input not taken this round (past the soft limit) carries over: the
       // batches by copy, the frontier records by position.
       int64_t next = (int64_t)std::min<unsigned long long>(c2[1], (unsigned long long)cap);
