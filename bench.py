@@ -361,6 +361,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk,
         "stats": {"pairs": npairs, "segment_pairs": units, "beta_retried": s_last["beta_retried"],
                   "retry_ms": s_last["ms_retry"], "front_records": s_last["bh_front_records"],
+                  "front_pairs_kept_far": s_last["bh_far_reused"], "front_pairs_opened": s_last["bh_far_subtracted"],
                   "retry_from_roots": s_last["bh_retry_from_roots"], "rounds": s_last["bh_rounds"],
                   "escalated": s_last["bh_escalated"], "wait_timeouts": s_last["bh_wait_timeouts"],
                   "fp64_recomputed": s_last["fp64_recomputed"], "tree_build_ms": s_last["ms_tree_build"],
