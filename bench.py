@@ -221,6 +221,8 @@ def run_ours(args, rank, world, local_rank):
     tune = None
     if args.bh_occupancy:
         prm.bh_occupancy = args.bh_occupancy
+    if args.fp64_margin is not None:
+        prm.fp64_margin = args.fp64_margin
     if args.bh_budget:
         prm.bh_budget = args.bh_budget
     elif args.autotune and args.method == "barneshut":
@@ -495,6 +497,8 @@ def main():
                     help="fixed Barnes-Hut round budget (skips the autotuner); 0 = tuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune the Barnes-Hut round budget on a sample of the pairs before timing")
+    ap.add_argument("--fp64-margin", type=float, default=None,
+                    help="margin to the rounding boundary below which a pair is recomputed in FP64 (default 0.25)")
     ap.add_argument("--bh-occupancy", type=int, default=0,
                     help="CTAs per SM of the traversal kernels (5, 6 or 7; 0 = the library's default or the "
                          "autotuner's choice)")

@@ -939,7 +939,17 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   int2 *spill = A.spill + (size_t)gw * kSpill;
   // Per-lane counts in 32 bits (a lane classifies at most one node pair per
   // step, and a launch's steps are bounded by its batches' budgets).
-  unsigned nfar = 0, nent = 0, nreuse = 0, nsub = 0;
+  unsigned nfar = 0, nent = 0;
+  // kCont: frontier pairs kept far and opened, counted in shared memory (they
+  // change once per frontier pair; registers are the traversal's limit).
+  __shared__ unsigned s_fcount[kWarps][kCont ? 2 : 1];
+  if constexpr (kCont) {
+    if (lane == 0) {
+      s_fcount[w][0] = 0;
+      s_fcount[w][1] = 0;
+    }
+    __syncwarp();
+  }
   // kFront: the warp's open frontier record, its fill and its slot, kept in
   // shared memory (read and written once per 32 far pairs) rather than in
   // registers across the traversal loop.
@@ -1010,9 +1020,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         if (x < cnt0) {
           v = src[x];
           keep = !(ratio[x] > clear);
-          nreuse += keep ? 0u : 1u;
         }
         const unsigned km = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_fcount[w][0] += (unsigned)(min(cnt0 - x0, 32) - __popc(km));
         v.x |= kFrontFlag;
         if (keep) stack[top + __popc(km & ((1u << lane) - 1))] = v;
         top += __popc(km);
@@ -1151,15 +1161,20 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
         // value; one that opens gives it back (subtract) and goes on.
         bool sub = false;
         if constexpr (kCont) {
+          bool kept = false;
           if (fpair) {
             if (kind == 2) {
               kind = 0;
-              nreuse += 1;
+              kept = true;
             } else {
               sub = true;
-              nsub += 1;
               fv.w = -fv.w;
             }
+          }
+          const unsigned km = __ballot_sync(0xffffffffu, kept), um = __ballot_sync(0xffffffffu, sub);
+          if (lane == 0) {
+            s_fcount[w][0] += (unsigned)__popc(km);
+            s_fcount[w][1] += (unsigned)__popc(um);
           }
         }
         const unsigned sm = __ballot_sync(0xffffffffu, kind == 3);
@@ -1291,7 +1306,8 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     atomicAdd(A.counts + 5, (double)nent);
   }
   if constexpr (kCont) {
-    const double wreuse = warp_sum_u32(nreuse), wsub = warp_sum_u32(nsub);
+    __syncwarp();
+    const double wreuse = (double)s_fcount[w][0], wsub = (double)s_fcount[w][1];
     if (lane == 0) {
       atomicAdd(A.counts + 6, wreuse);
       atomicAdd(A.counts + 7, wsub);
