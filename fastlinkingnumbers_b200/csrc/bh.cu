@@ -37,9 +37,10 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
-#include <cmath>
+#include <cstring>
 #include <numeric>
 #include <type_traits>
 
@@ -68,6 +69,10 @@ constexpr int kWarps = 4;          // warps per traversal CTA
 // reserved by the system.
 #ifndef FLN_BH_CARVEOUT
 #define FLN_BH_CARVEOUT 44
+#endif
+// Six and seven CTAs per SM (fln_params.bh_occupancy).
+#ifndef FLN_BH_CARVEOUT_6
+#define FLN_BH_CARVEOUT_6 58
 #endif
 constexpr int kStack = FLN_BH_STACK;
 constexpr int kSpill = 8192;       // global spill entries per warp
@@ -155,6 +160,63 @@ __device__ __forceinline__ NodeMom load_mom(const NodeMom *p) {
   unsigned long long *w = reinterpret_cast<unsigned long long *>(&m);
 #pragma unroll
   for (int i = 0; i < 4; ++i) load32(reinterpret_cast<const char *>(p) + 32 * i, w + 4 * i);
+  return m;
+}
+
+// Moment records of far pairs staged in shared memory by bulk copies (1) or
+// loaded by the lanes (0). A scattered 32-byte load costs the L1 data pipe
+// one wavefront per lane, and the moment records are about half of the
+// traversal's loads; a bulk copy of a record (cp.async.bulk, 128 bytes,
+// completion counted on an mbarrier) is done by the copy engine instead, and
+// the lanes then read the staged records from shared memory at 128 bytes per
+// wavefront. Slots are 144 bytes apart (16-byte aligned, as bulk copies
+// require), so chunk k of slot s sits in bank group (s + k) mod 8 and 8 lanes
+// reading the same chunk of 8 consecutive slots do not conflict.
+#ifndef FLN_BH_TMA_MOM
+#define FLN_BH_TMA_MOM 0
+#endif
+constexpr int kStagePairs = 16;            // far pairs per staged drain
+constexpr int kSlotF4 = 9;                 // slot stride in float4 (144 bytes)
+constexpr int kStageWaitPolls = 1 << 20;   // bounded wait on the staging barrier
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Waits for the barrier's phase of the given parity; false if it did not
+// complete within kStageWaitPolls tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (int i = 0; i < kStageWaitPolls; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// One 128-byte moment record into a shared-memory slot (both 16-byte aligned).
+__device__ __forceinline__ void bulk_record(void *dst, const NodeMom *src, uint64_t *bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"((uint32_t)sizeof(NodeMom)), "r"(smem_u32(bar))
+               : "memory");
+}
+// The record staged in slot s.
+__device__ __forceinline__ NodeMom stage_read(const float4 *stage, int s) {
+  NodeMom m;
+  float4 *d = reinterpret_cast<float4 *>(&m);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) d[k] = stage[kSlotF4 * s + k];
   return m;
 }
 
@@ -350,6 +412,49 @@ __device__ void leaf_build(const double *xyz, int64_t o, int64_t n, int32_t seg,
   const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
   for (int kk = 0; kk < 3; ++kk)
     for (int e = 0; e < 6; ++e) B.Q[6 * kk + e] = ((1.0 / 12.0) * B.t[kk]) * (B.t[ii[e]] * B.t[jj[e]]);
+}
+
+// Leaf records of the curve-order trees (thread per leaf), straight from the
+// segment's two vertices: the values finish_record forms from leaf_build's
+// record (box, midpoint, tangent c, C_D = 0, C_Q,k = c_k c c^T / 12), without
+// an FP64 build record in registers, so the kernel runs at full occupancy.
+__global__ void __launch_bounds__(256) build_leaves(TreeArgs A, const int64_t *seg_start2, int64_t total) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int k = find_loop_of(seg_start2, A.nloops, g);
+  const int l = A.loops[k];
+  const int64_t o = A.off[l], n = A.off[l + 1] - o;
+  const int64_t base = A.node_base[l];
+  const int32_t node = (int32_t)(n - 1 + (g - seg_start2[k]));
+  const int32_t seg = A.leaf_seg[base + node];
+  const int64_t v0 = o + seg, v1 = o + (seg + 1 == n ? 0 : seg + 1);
+  double t[3], d[3];
+  NodeHdr h;
+  NodeMom m;
+  for (int a = 0; a < 3; ++a) {
+    const double p0 = A.xyz[3 * v0 + a], p1 = A.xyz[3 * v1 + a];
+    t[a] = p1 - p0;
+    h.m[a] = 0.5 * p0 + 0.5 * p1;
+    d[a] = fmax(p0, p1) - fmin(p0, p1);
+  }
+  h.rsq = 0.25 * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  h.r = sqrt(h.rsq);
+  h.left = -1 - seg;
+  h.right = -1;
+  h.lo = seg;
+  h.cnt = 1;
+  const double tn = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  h.tn = (float)tn;
+  h.dn = 0.f;
+  for (int a = 0; a < 3; ++a) m.t[a] = (float)t[a];
+  for (int a = 0; a < 9; ++a) m.D[a] = 0.f;
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int kk = 0; kk < 3; ++kk)
+    for (int e = 0; e < 6; ++e) m.Q[6 * kk + e] = (float)(((1.0 / 12.0) * t[kk]) * (t[ii[e]] * t[jj[e]]));
+  m.qn = (float)(tn * tn * tn / 36.0);
+  m.pad = 0.f;
+  put16(&A.hdr[base + node], h);
+  put16(&A.mom[base + node], m);
 }
 
 // Thread per leaf: write the leaf's traversal record and walk up; the second
@@ -923,8 +1028,21 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   __shared__ float2 s_farr[kWarps][64];  // the two Eq. 14 weights (far_weights)
   __shared__ float s_fart[kWarps][kFront ? 64 : 1];  // separation ratios for the frontier (front_ratio)
   __shared__ std::conditional_t<kLearn, MlpFrag, int> s_mlp;
+  // Staged moment records (FLN_BH_TMA_MOM): node 1's in slots [0, 16), node
+  // 2's in [16, 32), one barrier per warp.
+  __shared__ __align__(128) float4 s_stage[kWarps][FLN_BH_TMA_MOM ? 2 * kStagePairs * kSlotF4 : 1];
+  __shared__ __align__(8) uint64_t s_mbar[kWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + w;
+  float4 *stage = s_stage[w];
+  uint64_t *mbar = &s_mbar[w];
+  uint32_t mphase = 0;
+  const bool staged = FLN_BH_TMA_MOM != 0;
+  bool sfail = false;  // a staging wait ran out (status 16)
+  if (staged) {
+    if (lane == 0) mbar_init(mbar, 1);
+    __syncwarp();
+  }
   int2 *stack = s_stack[w];
   int2 *farq = s_far[w];
   float4 *farv = s_farv[w];
@@ -964,6 +1082,7 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
   }
   const long long total = A.nin + A.nin1;
   for (;;) {
+    if (sfail) break;
     long long b = 0;
     if (lane == 0) {
       // Past the soft limit of the exact list this round takes no new batch
@@ -1248,8 +1367,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       // Far-field evaluation, 32 queued pairs at a time, and what is left
       // once the batch is done: the one far-field call site of the kernel
       // (a subtraction then gives back exactly what the first pass added).
-      while (nf >= 32 || (done && nf > 0)) {
-        const int m = min(nf, 32);
+      const int drain = staged ? kStagePairs : 32;
+      while (nf >= drain || (done && nf > 0)) {
+        const int m = min(nf, drain);
         int2 q = make_int2(0, 0);
         if (lane < m) q = farq[nf - m + lane];
         if constexpr (kFront) {
@@ -1262,11 +1382,30 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
           }
           __syncwarp();
         }
+        if (staged) {
+          if (lane == 0) mbar_expect(mbar, (uint32_t)(m * 2 * sizeof(NodeMom)));
+          __syncwarp();
+          if (lane < m) {
+            bulk_record(stage + kSlotF4 * lane, M1 + q.x, mbar);
+            bulk_record(stage + kSlotF4 * (kStagePairs + lane), M2 + q.y, mbar);
+          }
+          if (!__all_sync(0xffffffffu, mbar_wait(mbar, mphase))) {
+            sfail = true;
+            if (lane == 0) atomicOr(A.status, 16);
+            done = true;
+            break;
+          }
+          mphase ^= 1u;
+        }
         if (lane < m) {
           const float4 v = farv[nf - m + lane];
           const float2 rr = farr[nf - m + lane];  // Eq. 14 weights
           double fs = 0.0, fe = 0.0;
-          far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)fabsf(v.w), rr.x, rr.y, fs, fe);
+          if (staged)
+            far_eval(stage_read(stage, lane), stage_read(stage, kStagePairs + lane), v.x, v.y, v.z,
+                     (double)fabsf(v.w), rr.x, rr.y, fs, fe);
+          else
+            far_eval(load_mom(M1 + q.x), load_mom(M2 + q.y), v.x, v.y, v.z, (double)fabsf(v.w), rr.x, rr.y, fs, fe);
           if (v.w < 0.f) {
             sum -= fs;
             err -= fe;
@@ -1300,6 +1439,9 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
     __syncwarp();
     front_close(A, frec, ffill, fslot, lane);
   }
+  // A staging wait that ran out leaves copies in flight: give them another
+  // bounded wait before the CTA's shared memory is released.
+  if (sfail) mbar_wait(mbar, mphase);
   const double wfar = warp_sum_u32(nfar);
   if (lane == 0) {
     atomicAdd(A.counts, wfar);
@@ -1659,7 +1801,7 @@ struct TraverseSet {
   int carveout;   // shared-memory carveout (percent) that fits that many CTAs of 16 KB
 };
 const TraverseSet kTraverseSets[] = {{bh_traverse_o5, bh_traverse_front_o5, bh_traverse_cont_o5, 5, FLN_BH_CARVEOUT},
-                                     {bh_traverse_o6, bh_traverse_front_o6, bh_traverse_cont_o6, 6, 58},
+                                     {bh_traverse_o6, bh_traverse_front_o6, bh_traverse_cont_o6, 6, FLN_BH_CARVEOUT_6},
                                      {bh_traverse_o7, bh_traverse_front_o7, bh_traverse_cont_o7, 7, 58}};
 __global__ void __launch_bounds__(32 * kWarps) bh_traverse_record(TravArgs A) { traverse<false, true, 0>(A); }
 // The learned kernels at FLN_LEARNED_MIN_CTAS CTAs per SM: their MLP code
@@ -2584,7 +2726,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int, d_height, d_hcnt,
                                                                         d_range);
     identity_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
-    build_moments<<<(int)((tot_leaf + 127) / 128), 128, 0, st>>>(T, d_segall, tot_leaf, false);
+    build_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
     FLN_CUDA(cudaGetLastError());
     launches += 3;
     int32_t hcnt[64];
@@ -3037,6 +3179,8 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   if (status & 1)
     throw Error(FLN_ERR_STACK_OVERFLOW, "Barnes-Hut traversal stack exceeded its bound (depth " +
                                             std::to_string(maxdepth) + ").");
+  if (status & 16)
+    throw Error(FLN_ERR_INTERNAL, "Barnes-Hut moment staging did not complete within its bounded wait.");
   if (status != 0)
     throw Error(FLN_ERR_INTERNAL, "Barnes-Hut work list exceeded its capacity (status " + std::to_string(status) +
                                       ").");
