@@ -529,8 +529,14 @@ __global__ void bucket_heights(const uint8_t *height, int64_t total_internal, co
 // build of build_height; it writes no build record except for nodes whose
 // parent build_height builds. Most internal nodes are this low, so this
 // skips most of the 320-byte build records.
-__global__ void build_small(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count,
-                            const int2 *range) {
+// The passes: box; c_M and C_D (the header, the first 48 bytes of the moment
+// record and, for a node whose parent build_height builds, those fields of
+// its build record); then C_Q (the rest). Each pass re-reads the node's few
+// vertices (from L1) and accumulates its fields in the order of a single
+// pass, so the records are the same; only one pass's sums are live at a time
+// (the single-pass kernel held 124 registers).
+__global__ void __launch_bounds__(128) build_small(TreeArgs A, const int64_t *seg_start, const int32_t *bucket,
+                                                   int64_t count, const int2 *range) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const int64_t g = bucket[e];
@@ -543,48 +549,100 @@ __global__ void build_small(TreeArgs A, const int64_t *seg_start, const int32_t 
   const int32_t lo = rg.x, hi = rg.y & INT_MAX;
   const bool need = rg.y < 0;
   const double *V = A.xyz + 3 * o;
-  BuildNode P;
+  double blo[3], bhi[3], mid[3];
   for (int a = 0; a < 3; ++a) {
-    P.lo[a] = V[3 * lo + a];
-    P.hi[a] = P.lo[a];
+    blo[a] = V[3 * lo + a];
+    bhi[a] = blo[a];
   }
   for (int32_t v = lo + 1; v <= hi; ++v) {
     const int64_t w = v == n ? 0 : v;
     for (int a = 0; a < 3; ++a) {
       const double x = V[3 * w + a];
-      P.lo[a] = fmin(P.lo[a], x);
-      P.hi[a] = fmax(P.hi[a], x);
+      blo[a] = fmin(blo[a], x);
+      bhi[a] = fmax(bhi[a], x);
     }
   }
-  for (int a = 0; a < 3; ++a) {
-    P.mid[a] = 0.5 * (P.hi[a] + P.lo[a]);
-    P.t[a] = 0.0;
-  }
-  for (int a = 0; a < 9; ++a) P.D[a] = 0.0;
-  for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
-  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
-  for (int32_t sg = lo; sg < hi; ++sg) {
-    const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
-    double t[3], r[3];
-    for (int a = 0; a < 3; ++a) {
-      const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
-      t[a] = p1 - p0;
-      r[a] = (0.5 * p0 + 0.5 * p1) - P.mid[a];
-    }
-    for (int a = 0; a < 3; ++a) P.t[a] += t[a];
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) P.D[3 * a + b] += t[a] * r[b];
-    for (int kk = 0; kk < 3; ++kk)
-      for (int q = 0; q < 6; ++q) {
-        const int i = ii[q], j = jj[q];
-        P.Q[6 * kk + q] += ((1.0 / 12.0) * t[kk]) * (t[i] * t[j]) + t[kk] * (r[i] * r[j]);
+  for (int a = 0; a < 3; ++a) mid[a] = 0.5 * (bhi[a] + blo[a]);
+  NodeMom *M = A.mom + base + node;
+  BuildNode *B = A.bn + g;
+  {  // c_M and C_D
+    double t[3] = {0.0, 0.0, 0.0}, D[9];
+    for (int a = 0; a < 9; ++a) D[a] = 0.0;
+    for (int32_t sg = lo; sg < hi; ++sg) {
+      const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
+      double ts[3], r[3];
+      for (int a = 0; a < 3; ++a) {
+        const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
+        ts[a] = p1 - p0;
+        r[a] = (0.5 * p0 + 0.5 * p1) - mid[a];
       }
+      for (int a = 0; a < 3; ++a) t[a] += ts[a];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) D[3 * a + b] += ts[a] * r[b];
+    }
+    NodeHdr h;
+    const double dx = bhi[0] - blo[0], dy = bhi[1] - blo[1], dz = bhi[2] - blo[2];
+    h.m[0] = mid[0];
+    h.m[1] = mid[1];
+    h.m[2] = mid[2];
+    h.rsq = 0.25 * (dx * dx + dy * dy + dz * dz);
+    h.r = sqrt(h.rsq);
+    h.left = A.children[2 * (base + node)];
+    h.right = A.children[2 * (base + node) + 1];
+    h.lo = lo;
+    h.cnt = hi - lo;
+    double dd = 0;
+    for (int a = 0; a < 9; ++a) dd += D[a] * D[a];
+    h.tn = (float)sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    h.dn = (float)(sqrt(dd) * kInvRt3);
+    put16(A.hdr + base + node, h);
+    float4 *m4 = reinterpret_cast<float4 *>(M);
+    m4[0] = make_float4((float)t[0], (float)t[1], (float)t[2], (float)D[0]);
+    m4[1] = make_float4((float)D[1], (float)D[2], (float)D[3], (float)D[4]);
+    m4[2] = make_float4((float)D[5], (float)D[6], (float)D[7], (float)D[8]);
+    if (need) {
+      for (int a = 0; a < 3; ++a) {
+        B->lo[a] = blo[a];
+        B->hi[a] = bhi[a];
+        B->mid[a] = mid[a];
+        B->t[a] = t[a];
+      }
+      for (int a = 0; a < 9; ++a) B->D[a] = D[a];
+    }
   }
-  P.seg_lo = lo;
-  P.seg_cnt = hi - lo;
-  if (need) put16(A.bn + g, P);
-  const int32_t cl = A.children[2 * (base + node)], cr = A.children[2 * (base + node) + 1];
-  finish_record(P, A.hdr[base + node], A.mom[base + node], false, 0, cl, cr);
+  {  // C_Q
+    double Q[18];
+    for (int a = 0; a < 18; ++a) Q[a] = 0.0;
+    const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+    for (int32_t sg = lo; sg < hi; ++sg) {
+      const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
+      double t[3], r[3];
+      for (int a = 0; a < 3; ++a) {
+        const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
+        t[a] = p1 - p0;
+        r[a] = (0.5 * p0 + 0.5 * p1) - mid[a];
+      }
+      for (int kk = 0; kk < 3; ++kk)
+        for (int q = 0; q < 6; ++q) {
+          const int i = ii[q], j = jj[q];
+          Q[6 * kk + q] += ((1.0 / 12.0) * t[kk]) * (t[i] * t[j]) + t[kk] * (r[i] * r[j]);
+        }
+    }
+    double qq = 0;
+    for (int kk = 0; kk < 3; ++kk)
+      for (int q = 0; q < 6; ++q) qq += (q < 3 ? 1.0 : 2.0) * Q[6 * kk + q] * Q[6 * kk + q];
+    float4 *m4 = reinterpret_cast<float4 *>(M);
+    m4[3] = make_float4((float)Q[0], (float)Q[1], (float)Q[2], (float)Q[3]);
+    m4[4] = make_float4((float)Q[4], (float)Q[5], (float)Q[6], (float)Q[7]);
+    m4[5] = make_float4((float)Q[8], (float)Q[9], (float)Q[10], (float)Q[11]);
+    m4[6] = make_float4((float)Q[12], (float)Q[13], (float)Q[14], (float)Q[15]);
+    m4[7] = make_float4((float)Q[16], (float)Q[17], (float)(sqrt(qq) / 3.0), 0.f);
+    if (need) {
+      for (int a = 0; a < 18; ++a) B->Q[a] = Q[a];
+      B->seg_lo = lo;
+      B->seg_cnt = hi - lo;
+    }
+  }
 }
 
 __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count) {
