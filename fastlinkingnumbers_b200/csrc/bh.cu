@@ -265,9 +265,9 @@ __device__ __forceinline__ int32_t add_one_rank(int32_t *count, int32_t key, boo
 // seg_start[k] = sum of (n - 1) over the first k listed loops. With height
 // != nullptr it also records the node's height ceil(log2(range size)) (the
 // children of a node are always lower) and counts the nodes per height.
-__global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t total_internal, uint8_t *height,
-                                    int32_t *height_count, int2 *range) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t g0, int64_t total_internal,
+                                    uint8_t *height, int32_t *height_count, int2 *range) {
+  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (height) {  // every lane of the warp takes part in the counting
     int32_t h = 0;
     if (g < total_internal) {
@@ -321,8 +321,8 @@ __global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_
 
 // Leaves of every listed loop: leaf_seg is identity for curve-order trees
 // (the host fills it for kd trees).
-__global__ void identity_leaves(TreeArgs A, const int64_t *seg_start2, int64_t total) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void identity_leaves(TreeArgs A, const int64_t *seg_start2, int64_t g0, int64_t total) {
+  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
   const int k = find_loop_of(seg_start2, A.nloops, g);
   const int l = A.loops[k];
@@ -418,8 +418,9 @@ __device__ void leaf_build(const double *xyz, int64_t o, int64_t n, int32_t seg,
 // segment's two vertices: the values finish_record forms from leaf_build's
 // record (box, midpoint, tangent c, C_D = 0, C_Q,k = c_k c c^T / 12), without
 // an FP64 build record in registers, so the kernel runs at full occupancy.
-__global__ void __launch_bounds__(256) build_leaves(TreeArgs A, const int64_t *seg_start2, int64_t total) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) build_leaves(TreeArgs A, const int64_t *seg_start2, int64_t g0,
+                                                    int64_t total) {
+  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
   const int k = find_loop_of(seg_start2, A.nloops, g);
   const int l = A.loops[k];
@@ -513,9 +514,9 @@ __global__ void build_moments(TreeArgs A, const int64_t *seg_start2, int64_t tot
 // height, listed in bucket[0, count), each from its two children, which
 // earlier launches finished (leaves: rebuilt from their vertices). Same
 // arithmetic as the walk-up of build_moments, so the same records.
-__global__ void bucket_heights(const uint8_t *height, int64_t total_internal, const int32_t *height_off,
+__global__ void bucket_heights(const uint8_t *height, int64_t g0, int64_t total_internal, const int32_t *height_off,
                                int32_t *cursor, int32_t *bucket) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int32_t h = g < total_internal ? height[g] : 0;
   const int32_t r = add_one_rank(cursor, h, g < total_internal);
   if (g < total_internal) bucket[height_off[h] + r] = (int32_t)g;
@@ -529,14 +530,8 @@ __global__ void bucket_heights(const uint8_t *height, int64_t total_internal, co
 // build of build_height; it writes no build record except for nodes whose
 // parent build_height builds. Most internal nodes are this low, so this
 // skips most of the 320-byte build records.
-// The passes: box; c_M and C_D (the header, the first 48 bytes of the moment
-// record and, for a node whose parent build_height builds, those fields of
-// its build record); then C_Q (the rest). Each pass re-reads the node's few
-// vertices (from L1) and accumulates its fields in the order of a single
-// pass, so the records are the same; only one pass's sums are live at a time
-// (the single-pass kernel held 124 registers).
-__global__ void __launch_bounds__(128) build_small(TreeArgs A, const int64_t *seg_start, const int32_t *bucket,
-                                                   int64_t count, const int2 *range) {
+__global__ void build_small(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count,
+                            const int2 *range) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const int64_t g = bucket[e];
@@ -549,100 +544,48 @@ __global__ void __launch_bounds__(128) build_small(TreeArgs A, const int64_t *se
   const int32_t lo = rg.x, hi = rg.y & INT_MAX;
   const bool need = rg.y < 0;
   const double *V = A.xyz + 3 * o;
-  double blo[3], bhi[3], mid[3];
+  BuildNode P;
   for (int a = 0; a < 3; ++a) {
-    blo[a] = V[3 * lo + a];
-    bhi[a] = blo[a];
+    P.lo[a] = V[3 * lo + a];
+    P.hi[a] = P.lo[a];
   }
   for (int32_t v = lo + 1; v <= hi; ++v) {
     const int64_t w = v == n ? 0 : v;
     for (int a = 0; a < 3; ++a) {
       const double x = V[3 * w + a];
-      blo[a] = fmin(blo[a], x);
-      bhi[a] = fmax(bhi[a], x);
+      P.lo[a] = fmin(P.lo[a], x);
+      P.hi[a] = fmax(P.hi[a], x);
     }
   }
-  for (int a = 0; a < 3; ++a) mid[a] = 0.5 * (bhi[a] + blo[a]);
-  NodeMom *M = A.mom + base + node;
-  BuildNode *B = A.bn + g;
-  {  // c_M and C_D
-    double t[3] = {0.0, 0.0, 0.0}, D[9];
-    for (int a = 0; a < 9; ++a) D[a] = 0.0;
-    for (int32_t sg = lo; sg < hi; ++sg) {
-      const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
-      double ts[3], r[3];
-      for (int a = 0; a < 3; ++a) {
-        const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
-        ts[a] = p1 - p0;
-        r[a] = (0.5 * p0 + 0.5 * p1) - mid[a];
-      }
-      for (int a = 0; a < 3; ++a) t[a] += ts[a];
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) D[3 * a + b] += ts[a] * r[b];
-    }
-    NodeHdr h;
-    const double dx = bhi[0] - blo[0], dy = bhi[1] - blo[1], dz = bhi[2] - blo[2];
-    h.m[0] = mid[0];
-    h.m[1] = mid[1];
-    h.m[2] = mid[2];
-    h.rsq = 0.25 * (dx * dx + dy * dy + dz * dz);
-    h.r = sqrt(h.rsq);
-    h.left = A.children[2 * (base + node)];
-    h.right = A.children[2 * (base + node) + 1];
-    h.lo = lo;
-    h.cnt = hi - lo;
-    double dd = 0;
-    for (int a = 0; a < 9; ++a) dd += D[a] * D[a];
-    h.tn = (float)sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-    h.dn = (float)(sqrt(dd) * kInvRt3);
-    put16(A.hdr + base + node, h);
-    float4 *m4 = reinterpret_cast<float4 *>(M);
-    m4[0] = make_float4((float)t[0], (float)t[1], (float)t[2], (float)D[0]);
-    m4[1] = make_float4((float)D[1], (float)D[2], (float)D[3], (float)D[4]);
-    m4[2] = make_float4((float)D[5], (float)D[6], (float)D[7], (float)D[8]);
-    if (need) {
-      for (int a = 0; a < 3; ++a) {
-        B->lo[a] = blo[a];
-        B->hi[a] = bhi[a];
-        B->mid[a] = mid[a];
-        B->t[a] = t[a];
-      }
-      for (int a = 0; a < 9; ++a) B->D[a] = D[a];
-    }
+  for (int a = 0; a < 3; ++a) {
+    P.mid[a] = 0.5 * (P.hi[a] + P.lo[a]);
+    P.t[a] = 0.0;
   }
-  {  // C_Q
-    double Q[18];
-    for (int a = 0; a < 18; ++a) Q[a] = 0.0;
-    const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
-    for (int32_t sg = lo; sg < hi; ++sg) {
-      const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
-      double t[3], r[3];
-      for (int a = 0; a < 3; ++a) {
-        const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
-        t[a] = p1 - p0;
-        r[a] = (0.5 * p0 + 0.5 * p1) - mid[a];
-      }
-      for (int kk = 0; kk < 3; ++kk)
-        for (int q = 0; q < 6; ++q) {
-          const int i = ii[q], j = jj[q];
-          Q[6 * kk + q] += ((1.0 / 12.0) * t[kk]) * (t[i] * t[j]) + t[kk] * (r[i] * r[j]);
-        }
+  for (int a = 0; a < 9; ++a) P.D[a] = 0.0;
+  for (int a = 0; a < 18; ++a) P.Q[a] = 0.0;
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int32_t sg = lo; sg < hi; ++sg) {
+    const int64_t w0 = sg, w1 = sg + 1 == n ? 0 : sg + 1;
+    double t[3], r[3];
+    for (int a = 0; a < 3; ++a) {
+      const double p0 = V[3 * w0 + a], p1 = V[3 * w1 + a];
+      t[a] = p1 - p0;
+      r[a] = (0.5 * p0 + 0.5 * p1) - P.mid[a];
     }
-    double qq = 0;
+    for (int a = 0; a < 3; ++a) P.t[a] += t[a];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) P.D[3 * a + b] += t[a] * r[b];
     for (int kk = 0; kk < 3; ++kk)
-      for (int q = 0; q < 6; ++q) qq += (q < 3 ? 1.0 : 2.0) * Q[6 * kk + q] * Q[6 * kk + q];
-    float4 *m4 = reinterpret_cast<float4 *>(M);
-    m4[3] = make_float4((float)Q[0], (float)Q[1], (float)Q[2], (float)Q[3]);
-    m4[4] = make_float4((float)Q[4], (float)Q[5], (float)Q[6], (float)Q[7]);
-    m4[5] = make_float4((float)Q[8], (float)Q[9], (float)Q[10], (float)Q[11]);
-    m4[6] = make_float4((float)Q[12], (float)Q[13], (float)Q[14], (float)Q[15]);
-    m4[7] = make_float4((float)Q[16], (float)Q[17], (float)(sqrt(qq) / 3.0), 0.f);
-    if (need) {
-      for (int a = 0; a < 18; ++a) B->Q[a] = Q[a];
-      B->seg_lo = lo;
-      B->seg_cnt = hi - lo;
-    }
+      for (int q = 0; q < 6; ++q) {
+        const int i = ii[q], j = jj[q];
+        P.Q[6 * kk + q] += ((1.0 / 12.0) * t[kk]) * (t[i] * t[j]) + t[kk] * (r[i] * r[j]);
+      }
   }
+  P.seg_lo = lo;
+  P.seg_cnt = hi - lo;
+  if (need) put16(A.bn + g, P);
+  const int32_t cl = A.children[2 * (base + node)], cr = A.children[2 * (base + node) + 1];
+  finish_record(P, A.hdr[base + node], A.mom[base + node], false, 0, cl, cr);
 }
 
 __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t *bucket, int64_t count) {
@@ -2749,6 +2692,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaEventRecord(ctx.ev2, st));
   if (prm.bh_tree == 1) {
     // The reference's kd-median tree, built on the host from a copy of the loops.
+    wait_xyz_pieces(ctx);
     std::vector<int32_t> ch_all(2 * nodes, 0), ls_all(nodes, 0);
     std::vector<double> xyz_host(3 * h_off.back());
     FLN_CUDA(cudaMemcpyAsync(xyz_host.data(), d_xyz, xyz_host.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -2779,40 +2723,65 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     int32_t *d_hoff = d_hcnt + 64, *d_hcur = d_hcnt + 128;
     int32_t *d_bucket = ctx.d_bh[19].as<int32_t>(std::max<int64_t>(tot_int, 1));
     int2 *d_range = ctx.d_bh[22].as<int2>(std::max<int64_t>(tot_int, 1));
-    FLN_CUDA(cudaMemsetAsync(d_hcnt, 0, 3 * 64 * sizeof(int32_t), st));
-    if (tot_int > 0)
-      curve_tree_topology<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(T, d_segint, tot_int, d_height, d_hcnt,
-                                                                        d_range);
-    identity_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
-    build_leaves<<<(int)((tot_leaf + 255) / 256), 256, 0, st>>>(T, d_segall, tot_leaf);
-    FLN_CUDA(cudaGetLastError());
-    launches += 3;
-    int32_t hcnt[64];
-    FLN_CUDA(cudaMemcpyAsync(hcnt, d_hcnt, sizeof hcnt, cudaMemcpyDeviceToHost, st));
-    FLN_CUDA(cudaStreamSynchronize(st));
-    int32_t hoff[64];
-    int32_t acc = 0;
-    for (int h = 0; h < 64; ++h) {
-      hoff[h] = acc;
-      acc += hcnt[h];
+    // The loops in groups: one per piece of the vertices still arriving from
+    // the host (each group's build waits only for its piece), else one.
+    std::vector<int32_t> group_end;  // loop index (into `loops`) where each group ends
+    std::vector<int> group_piece;
+    if (ctx.xyz_pieces > 0) {
+      int32_t k = 0;
+      for (int i = 0; i < ctx.xyz_pieces; ++i) {
+        while (k < nloops && h_off[loops[k] + 1] <= ctx.xyz_piece_end[i]) ++k;
+        group_end.push_back(k);
+        group_piece.push_back(i);
+      }
+      group_end.back() = nloops;
+    } else {
+      group_end.push_back(nloops);
+      group_piece.push_back(-1);
     }
-    if (tot_int > 0) {
-      FLN_CUDA(cudaMemcpyAsync(d_hoff, hoff, sizeof hoff, cudaMemcpyHostToDevice, st));
-      bucket_heights<<<(int)((tot_int + 255) / 256), 256, 0, st>>>(d_height, tot_int, d_hoff, d_hcur, d_bucket);
-      ++launches;
-      const int64_t nsmall = (int64_t)hoff[kSmallHeight + 1] - hoff[1];  // heights 1..kSmallHeight
-      if (nsmall > 0) {
-        build_small<<<(int)((nsmall + 127) / 128), 128, 0, st>>>(T, d_segint, d_bucket + hoff[1], nsmall, d_range);
-        ++launches;
-      }
-      for (int h = kSmallHeight + 1; h < 64; ++h) {
-        if (!hcnt[h]) continue;
-        build_height<<<(hcnt[h] + 127) / 128, 128, 0, st>>>(T, d_segint, d_bucket + hoff[h], hcnt[h]);
-        ++launches;
-      }
+    int32_t k0 = 0;
+    for (size_t gi = 0; gi < group_end.size(); ++gi) {
+      const int32_t k1 = group_end[gi];
+      if (group_piece[gi] >= 0) FLN_CUDA(cudaStreamWaitEvent(st, ctx.ev_piece[group_piece[gi]], 0));
+      if (k1 <= k0) continue;
+      const int64_t i0 = seg_int[k0], i1 = seg_int[k1], f0 = seg_all[k0], f1 = seg_all[k1];
+      FLN_CUDA(cudaMemsetAsync(d_hcnt, 0, 3 * 64 * sizeof(int32_t), st));
+      if (i1 > i0)
+        curve_tree_topology<<<(int)((i1 - i0 + 255) / 256), 256, 0, st>>>(T, d_segint, i0, i1, d_height, d_hcnt,
+                                                                          d_range);
+      identity_leaves<<<(int)((f1 - f0 + 255) / 256), 256, 0, st>>>(T, d_segall, f0, f1);
+      build_leaves<<<(int)((f1 - f0 + 255) / 256), 256, 0, st>>>(T, d_segall, f0, f1);
       FLN_CUDA(cudaGetLastError());
+      launches += 3;
+      int32_t hcnt[64];
+      FLN_CUDA(cudaMemcpyAsync(hcnt, d_hcnt, sizeof hcnt, cudaMemcpyDeviceToHost, st));
+      FLN_CUDA(cudaStreamSynchronize(st));
+      int32_t hoff[64];
+      int64_t acc = i0;  // this group's nodes fill bucket[i0, i1)
+      for (int h = 0; h < 64; ++h) {
+        hoff[h] = (int32_t)acc;
+        acc += hcnt[h];
+      }
+      if (i1 > i0) {
+        FLN_CUDA(cudaMemcpyAsync(d_hoff, hoff, sizeof hoff, cudaMemcpyHostToDevice, st));
+        bucket_heights<<<(int)((i1 - i0 + 255) / 256), 256, 0, st>>>(d_height, i0, i1, d_hoff, d_hcur, d_bucket);
+        ++launches;
+        const int64_t nsmall = (int64_t)hoff[kSmallHeight + 1] - hoff[1];  // heights 1..kSmallHeight
+        if (nsmall > 0) {
+          build_small<<<(int)((nsmall + 127) / 128), 128, 0, st>>>(T, d_segint, d_bucket + hoff[1], nsmall, d_range);
+          ++launches;
+        }
+        for (int h = kSmallHeight + 1; h < 64; ++h) {
+          if (!hcnt[h]) continue;
+          build_height<<<(hcnt[h] + 127) / 128, 128, 0, st>>>(T, d_segint, d_bucket + hoff[h], hcnt[h]);
+          ++launches;
+        }
+        FLN_CUDA(cudaGetLastError());
+      }
+      k0 = k1;
     }
   }
+  wait_xyz_pieces(ctx);  // the traversal reads every loop's vertices
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
   ctx.stats.ms_tree_build = ctx.elapsed(ctx.ev2, ctx.ev3);
 

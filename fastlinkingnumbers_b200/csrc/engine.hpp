@@ -109,6 +109,15 @@ struct Context {
   HostBuf h_in, h_out;  // pinned staging of copy_h2d / copy_d2h
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   cudaEvent_t ev_bk[2] = {nullptr, nullptr};  // around each exact-list launch
+  // Vertices from host arrays arrive in pieces on a copy stream (split at
+  // loop boundaries); the Barnes–Hut tree build of each piece's loops waits
+  // only for its piece. xyz_pieces = 0: the vertices are resident.
+  static constexpr int kXyzPieces = 4;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_piece[kXyzPieces] = {};
+  cudaEvent_t ev_before_copy = nullptr;
+  int64_t xyz_piece_end[kXyzPieces] = {};  // vertex index at which each piece ends
+  int xyz_pieces = 0;
   // Learned criterion in use on this context, and training buffers.
   DevBuf d_mlp, d_learn[8];
   // Device Discretize (discretize.cu).
@@ -126,6 +135,13 @@ struct Context {
   }
   ~Context();
 };
+
+// The context's stream waits for every piece of the vertices still on its
+// way (Context::xyz_pieces); afterwards they are resident.
+inline void wait_xyz_pieces(Context &c) {
+  for (int i = 0; i < c.xyz_pieces; ++i) cudaStreamWaitEvent(c.stream, c.ev_piece[i], 0);
+  c.xyz_pieces = 0;
+}
 
 // Mixed direct sum: a segment pair whose closest endpoint distance is below
 // this multiple of the longer segment's length is evaluated in FP64 (the
