@@ -112,7 +112,7 @@ struct Context {
   // Vertices from host arrays arrive in pieces on a copy stream (split at
   // loop boundaries); the Barnes–Hut tree build of each piece's loops waits
   // only for its piece. xyz_pieces = 0: the vertices are resident.
-  static constexpr int kXyzPieces = 4;
+  static constexpr int kXyzPieces = 8;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_piece[kXyzPieces] = {};
   cudaEvent_t ev_before_copy = nullptr;

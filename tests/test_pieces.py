@@ -15,7 +15,7 @@ def test_pinned_vertices_in_pieces_match_device_arrays():
     torch = pytest.importorskip("torch")
     eng = Engine(0)
     off, xyz, pairs = workloads.walk_pairs(seed=21, n_pairs=16, n_steps=100_000)
-    assert xyz.nbytes >= 64 << 20 and len(off) - 1 >= 4  # large enough to go in pieces
+    assert xyz.nbytes >= 64 << 20 and len(off) - 1 >= 8  # large enough to go in pieces
     h_xyz = torch.from_numpy(np.ascontiguousarray(xyz)).pin_memory().numpy()
     lk_h, err_h, fl_h = eng.linking_numbers(h_xyz, off, pairs, "barneshut")
     d_xyz = torch.from_numpy(np.ascontiguousarray(xyz)).cuda()
