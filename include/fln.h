@@ -213,9 +213,10 @@ fln_status fln_linking_numbers_device(fln_ctx *ctx, const double *d_xyz,
  * reads the plan's size and status back to the host, so it blocks the
  * calling thread until the work queued earlier on `stream` and a small
  * planning kernel have finished; it returns with the sums still in flight
- * on `stream`. The first call on a device looks up the array's device
- * address, so make it before any stream capture. Calls share the array:
- * calls whose work overlaps on the GPU race, so issue them one at a time. */
+ * on `stream`. Because every call waits on the host, no call can be
+ * captured into a CUDA graph (capture the surrounding work around it
+ * instead). Calls share the array: calls whose work overlaps on the GPU
+ * race, so issue them one at a time. */
 fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, const int64_t *d_loop_offsets,
                                               int32_t nloops, const int32_t *d_pairs, int64_t npairs,
                                               int32_t precision, double *d_lk_out, void *stream);
