@@ -18,9 +18,9 @@ Two steps, so that a long workload can run over several GPU calls:
 
   # on the GPU: FP64 direct sum of parts [a, b) of K work-balanced parts
   python tests/golden/make_config_certs.py run --config polymer --parts 8 \
-      --range 0:8 --out gpurun_out/fixtures
+      --range 0:8 --out /tmp/fixtures
   # anywhere: check and merge the parts into tests/golden/configs/
-  python tests/golden/make_config_certs.py merge --config polymer --src gpurun_out/fixtures
+  python tests/golden/make_config_certs.py merge --config polymer --src /tmp/fixtures
 
 The workloads are seeded (workloads.named); the digest pins the prepared
 polylines and pairs, so the test that reads these fixtures first checks that
