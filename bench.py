@@ -20,6 +20,7 @@ each step a seeded sample of the same workload's pairs.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -86,11 +87,16 @@ def make_workload(name: str, seed: int, loops: int = 200, steps: int = 50000, en
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """nvidia-smi clocks/throttle sampling during the timed region.
+
+    nvidia-smi is started before the warm-up steps (its start-up competes with
+    the process's own driver calls), and only the samples whose timestamps
+    fall between mark() and stop() are kept (all of them if none does)."""
 
     def __init__(self, index: int):
         self.path = tempfile.mktemp(suffix=".csv")
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        self.t0 = None
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
@@ -100,32 +106,43 @@ class ClockSampler:
         except Exception:
             self.p = None
 
+    def mark(self):
+        """The timed region starts now."""
+        self.t0 = datetime.datetime.now()
+
     def stop(self):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t1 = datetime.datetime.now()
         self.p.terminate()
         try:
             self.p.wait(5)
         except Exception:
             self.p.kill()
-        sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                sm_mhz, max_mhz = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for k, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(k)
+            try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+            except ValueError:
+                ts = None
+            rows.append((ts, sm_mhz, max_mhz, [k for k, v in zip(names, parts[6:10]) if v.lower() == "active"]))
         os.unlink(self.path)
+        inside = [r for r in rows if self.t0 is not None and r[0] is not None and self.t0 <= r[0] <= t1]
+        use = inside or rows
+        sm = [r[1] for r in use]
+        mx = [r[2] for r in use]
+        reasons = sorted({k for r in use for k in r[3]})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(sm), "samples_in_timed_region": len(inside)}
 
 
 def cpu_sample_run(poff, pxyz, pairs, target_s: float, seed: int, nthreads: int, oracle=None):
@@ -247,6 +264,7 @@ def run_ours(args, rank, world, local_rank):
                                    d_flags.data_ptr(), method=args.method, params=prm)
         return eng.stats()
 
+    clocks = ClockSampler(local_rank)
     for w in range(args.warmup):
         t0 = time.perf_counter()
         s = step()
@@ -258,9 +276,9 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(local_rank)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    clocks.mark()
     ev0.record(stream)
     st = []
     for _ in range(args.steps):

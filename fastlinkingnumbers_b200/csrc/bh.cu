@@ -910,11 +910,12 @@ __device__ __forceinline__ void load3(const double *xyz, int64_t v, double *p) {
 }
 
 // Traversal steps a warp takes on one batch per round before it hands the
-// rest of its stack on as new batches. Traversal time of the 14M-segment
-// polymer step on B200: 128 -> 208.2 ms, 256 -> 207.4 ms, 512 -> 222.5 ms,
-// 1024 -> 240.2 ms.
+// rest of its stack on as new batches (fln_params.bh_budget 0: this).
+// Traversal time of the 14M-segment polymer step on B200, leaf pairs only:
+// 128 -> 208.2 ms, 256 -> 207.4 ms, 512 -> 222.5 ms, 1024 -> 240.2 ms; with
+// the exact list, 128 -> 48.0 ms and 256 -> 49.6 ms.
 #ifndef FLN_BH_BUDGET
-#define FLN_BH_BUDGET 256
+#define FLN_BH_BUDGET kDefaultBhBudget
 #endif
 // Software prefetch of node records (generic addresses; the records are
 // valid device memory). Bit 0: the next step's headers into L1; bit 1: the

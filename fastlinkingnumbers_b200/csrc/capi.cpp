@@ -806,7 +806,7 @@ fln_status fln_autotune_direct(fln_ctx *ctx, const double *xyz, const int64_t *l
       }
     }
     r.best_direct_tile = best.direct_tile;
-    r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
+    r.best_budget = best.bh_budget > 0 ? best.bh_budget : kDefaultBhBudget;
     r.best_beta = best.barnes_hut_init_beta;
     r.best_bucket = best.bh_bucket > 0 ? best.bh_bucket : 8;
     r.best_occupancy = best.bh_occupancy > 0 ? best.bh_occupancy : 5;
@@ -903,7 +903,8 @@ fln_status fln_autotune(fln_ctx *ctx, const double *xyz, const int64_t *loop_off
         }
       }
     }
-    r.best_budget = best.bh_budget > 0 ? best.bh_budget : 256;
+    if (best.bh_budget <= 0) best.bh_budget = kDefaultBhBudget;  // the tuned parameters name their budget
+    r.best_budget = best.bh_budget;
     r.best_beta = best.barnes_hut_init_beta;
     r.best_bucket = best.bh_bucket > 0 ? best.bh_bucket : 8;
     r.best_occupancy = best.bh_occupancy > 0 ? best.bh_occupancy : 5;

@@ -89,7 +89,7 @@ typedef struct fln_params {
   int32_t host_prepare;         /* fln_certificate_compute: 0 = Discretize and the potential-link searches
                                    on the context's GPU (default), 1 = on the host; same output bit for bit */
   int32_t bh_budget;            /* traversal steps a warp spends on a batch per launch before handing the
-                                   rest on; 0 = 256. The node pairs stay the same; only the grouping of
+                                   rest on; 0 = 128. The node pairs stay the same; only the grouping of
                                    the FP64 partial sums changes (last-bit differences). */
   int32_t bh_bucket;            /* curve-order trees, bh_schedule 0: a node pair that is neither far nor a
                                    leaf pair and has at most this many segments a side is summed exactly,
