@@ -247,6 +247,25 @@ __device__ __forceinline__ int find_loop_of(const int64_t *start, int n, int64_t
   return lo;
 }
 
+// The listed loop of index x, for a block whose threads take the consecutive
+// indices [first, last]: two threads search the whole list for the block's
+// first and last index, and every thread then searches only between the two
+// (a block crosses few loop boundaries). Every thread of the block must call
+// it once (it synchronises the block).
+__device__ __forceinline__ int block_loop_of(const int64_t *start, int n, int64_t first, int64_t last, int64_t x) {
+  __shared__ int s_range[2];
+  if (threadIdx.x == 0) s_range[0] = find_loop_of(start, n, first);
+  if (threadIdx.x == (blockDim.x > 1 ? 1 : 0)) s_range[1] = find_loop_of(start, n, last);
+  __syncthreads();
+  int lo = s_range[0], hi = s_range[1] + 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (start[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // count[key] += 1 for the calling lane, one atomic per distinct key of the
 // warp; returns the count before the warp's run plus the lane's rank among
 // the lanes of the warp with its key.
@@ -267,11 +286,12 @@ __device__ __forceinline__ int32_t add_one_rank(int32_t *count, int32_t key, boo
 // children of a node are always lower) and counts the nodes per height.
 __global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_t g0, int64_t total_internal,
                                     uint8_t *height, int32_t *height_count, int2 *range) {
-  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t first = g0 + (int64_t)blockIdx.x * blockDim.x, g = first + threadIdx.x;
+  const int64_t last = min(first + (int64_t)blockDim.x, total_internal) - 1;
+  const int k = block_loop_of(seg_start, A.nloops, first, last, min(g, last));
   if (height) {  // every lane of the warp takes part in the counting
     int32_t h = 0;
     if (g < total_internal) {
-      const int k = find_loop_of(seg_start, A.nloops, g);
       const int l = A.loops[k];
       const int64_t n = A.off[l + 1] - A.off[l];
       const int64_t s = g - seg_start[k] + 1;
@@ -288,7 +308,6 @@ __global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_
     add_one_rank(height_count, h, g < total_internal);
   }
   if (g >= total_internal) return;
-  const int k = find_loop_of(seg_start, A.nloops, g);
   const int l = A.loops[k];
   const int64_t n = A.off[l + 1] - A.off[l];
   const int32_t node = (int32_t)(g - seg_start[k]);  // local internal id
@@ -317,18 +336,6 @@ __global__ void curve_tree_topology(TreeArgs A, const int64_t *seg_start, int64_
   A.parent[base + left] = node;
   A.parent[base + right] = node;
   A.arrive[base + node] = 0;
-}
-
-// Leaves of every listed loop: leaf_seg is identity for curve-order trees
-// (the host fills it for kd trees).
-__global__ void identity_leaves(TreeArgs A, const int64_t *seg_start2, int64_t g0, int64_t total) {
-  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= total) return;
-  const int k = find_loop_of(seg_start2, A.nloops, g);
-  const int l = A.loops[k];
-  const int64_t n = A.off[l + 1] - A.off[l];
-  const int64_t p = g - seg_start2[k];
-  A.leaf_seg[A.node_base[l] + n - 1 + p] = (int32_t)p;
 }
 
 // Reads a record written by another thread of this launch: L2 loads (the
@@ -420,14 +427,18 @@ __device__ void leaf_build(const double *xyz, int64_t o, int64_t n, int32_t seg,
 // an FP64 build record in registers, so the kernel runs at full occupancy.
 __global__ void __launch_bounds__(256) build_leaves(TreeArgs A, const int64_t *seg_start2, int64_t g0,
                                                     int64_t total) {
-  const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t first = g0 + (int64_t)blockIdx.x * blockDim.x, g = first + threadIdx.x;
+  const int64_t last = min(first + (int64_t)blockDim.x, total) - 1;
+  const int k = block_loop_of(seg_start2, A.nloops, first, last, min(g, last));
   if (g >= total) return;
-  const int k = find_loop_of(seg_start2, A.nloops, g);
   const int l = A.loops[k];
   const int64_t o = A.off[l], n = A.off[l + 1] - o;
   const int64_t base = A.node_base[l];
-  const int32_t node = (int32_t)(n - 1 + (g - seg_start2[k]));
-  const int32_t seg = A.leaf_seg[base + node];
+  // Curve order: leaf position p holds segment p (the identity leaf map,
+  // written here for build_height).
+  const int32_t seg = (int32_t)(g - seg_start2[k]);
+  const int32_t node = (int32_t)(n - 1 + seg);
+  A.leaf_seg[base + node] = seg;
   const int64_t v0 = o + seg, v1 = o + (seg + 1 == n ? 0 : seg + 1);
   double t[3], d[3];
   NodeHdr h;
@@ -2750,10 +2761,9 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       if (i1 > i0)
         curve_tree_topology<<<(int)((i1 - i0 + 255) / 256), 256, 0, st>>>(T, d_segint, i0, i1, d_height, d_hcnt,
                                                                           d_range);
-      identity_leaves<<<(int)((f1 - f0 + 255) / 256), 256, 0, st>>>(T, d_segall, f0, f1);
       build_leaves<<<(int)((f1 - f0 + 255) / 256), 256, 0, st>>>(T, d_segall, f0, f1);
       FLN_CUDA(cudaGetLastError());
-      launches += 3;
+      launches += 2;
       int32_t hcnt[64];
       FLN_CUDA(cudaMemcpyAsync(hcnt, d_hcnt, sizeof hcnt, cudaMemcpyDeviceToHost, st));
       FLN_CUDA(cudaStreamSynchronize(st));
