@@ -530,7 +530,8 @@ __global__ void bucket_heights(const uint8_t *height, int64_t g0, int64_t total_
   const int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int32_t h = g < total_internal ? height[g] : 0;
   const int32_t r = add_one_rank(cursor, h, g < total_internal);
-  if (g < total_internal) bucket[height_off[h] + r] = (int32_t)g;
+  const int64_t pos = (int64_t)height_off[h] + r;
+  if (g < total_internal && pos < total_internal) bucket[pos] = (int32_t)g;  // a count mismatch is caught on the host
 }
 
 // Nodes of height 1..kSmallHeight (at most 2^kSmallHeight segments), one
@@ -546,6 +547,7 @@ __global__ void build_small(TreeArgs A, const int64_t *seg_start, const int32_t 
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const int64_t g = bucket[e];
+  if (g < 0 || g >= seg_start[A.nloops]) return;  // only after a height-count mismatch, which the host reports
   const int k = find_loop_of(seg_start, A.nloops, g);
   const int l = A.loops[k];
   const int64_t o = A.off[l], n = A.off[l + 1] - o;
@@ -603,6 +605,7 @@ __global__ void build_height(TreeArgs A, const int64_t *seg_start, const int32_t
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const int64_t g = bucket[e];
+  if (g < 0 || g >= seg_start[A.nloops]) return;  // only after a height-count mismatch, which the host reports
   const int k = find_loop_of(seg_start, A.nloops, g);
   const int l = A.loops[k];
   const int64_t o = A.off[l], n = A.off[l + 1] - o;
@@ -1808,6 +1811,35 @@ FLN_TRAVERSE_KERNELS(5)
 FLN_TRAVERSE_KERNELS(6)
 FLN_TRAVERSE_KERNELS(7)
 
+// Internal nodes per height of the curve-order tree of an n-segment loop,
+// added to hcnt[64]: the split of curve_tree_topology ([lo, hi) -> [lo, mid),
+// [mid, hi), mid = lo + (hi - lo) / 2; a node of m >= 2 segments has height
+// ceil(log2 m)). The ranges of one depth have at most two sizes, so this takes
+// O(log n) steps. The host sizes the height launches from it without reading
+// the device's counts back first; the device's counts are checked against it
+// after the build.
+void curve_height_counts(int64_t n, int64_t *hcnt) {
+  std::vector<std::pair<int64_t, int64_t>> cur{{n, 1}}, next;
+  while (!cur.empty()) {
+    next.clear();
+    for (const auto &mc : cur) {
+      const int64_t m = mc.first, c = mc.second;
+      if (m < 2) continue;
+      hcnt[64 - __builtin_clzll((unsigned long long)(m - 1))] += c;
+      for (const int64_t sz : {m / 2, m - m / 2}) {
+        bool merged = false;
+        for (auto &x : next)
+          if (x.first == sz) {
+            x.second += c;
+            merged = true;
+          }
+        if (!merged) next.push_back({sz, c});
+      }
+    }
+    cur.swap(next);
+  }
+}
+
 struct TraverseSet {
   void (*plain)(TravArgs), (*front)(TravArgs), (*cont)(TravArgs);
   int ctas;       // CTAs per SM the set is built for
@@ -2731,8 +2763,11 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     // Curve-order trees: topology with node heights, leaf records, then one
     // launch per height (no arrival counters, no serial walk-up chains).
     uint8_t *d_height = ctx.d_bh[20].as<uint8_t>(std::max<int64_t>(tot_int, 1));
-    int32_t *d_hcnt = ctx.d_bh[18].as<int32_t>(3 * 64);
-    int32_t *d_hoff = d_hcnt + 64, *d_hcur = d_hcnt + 128;
+    // Per group: the device's height counts (checked after the build), then
+    // the height offsets and cursors of bucket_heights.
+    const int max_groups = std::max(ctx.xyz_pieces, 1);
+    int32_t *d_hcnt = ctx.d_bh[18].as<int32_t>((size_t)64 * max_groups + 128);
+    int32_t *d_hoff = d_hcnt + 64 * max_groups, *d_hcur = d_hoff + 64;
     int32_t *d_bucket = ctx.d_bh[19].as<int32_t>(std::max<int64_t>(tot_int, 1));
     int2 *d_range = ctx.d_bh[22].as<int2>(std::max<int64_t>(tot_int, 1));
     // The loops in groups: one per piece of the vertices still arriving from
@@ -2751,30 +2786,34 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       group_end.push_back(nloops);
       group_piece.push_back(-1);
     }
+    FLN_CUDA(cudaMemsetAsync(d_hcnt, 0, (size_t)64 * max_groups * sizeof(int32_t), st));
+    std::vector<int64_t> host_counts((size_t)64 * group_end.size(), 0);
+    std::vector<int32_t> hoff_all((size_t)64 * group_end.size(), 0);  // lives until the stream has read it
     int32_t k0 = 0;
     for (size_t gi = 0; gi < group_end.size(); ++gi) {
       const int32_t k1 = group_end[gi];
       if (group_piece[gi] >= 0) FLN_CUDA(cudaStreamWaitEvent(st, ctx.ev_piece[group_piece[gi]], 0));
       if (k1 <= k0) continue;
       const int64_t i0 = seg_int[k0], i1 = seg_int[k1], f0 = seg_all[k0], f1 = seg_all[k1];
-      FLN_CUDA(cudaMemsetAsync(d_hcnt, 0, 3 * 64 * sizeof(int32_t), st));
+      int64_t *hc = host_counts.data() + 64 * gi;
+      for (int32_t k = k0; k < k1; ++k) curve_height_counts(h_off[loops[k] + 1] - h_off[loops[k]], hc);
       if (i1 > i0)
-        curve_tree_topology<<<(int)((i1 - i0 + 255) / 256), 256, 0, st>>>(T, d_segint, i0, i1, d_height, d_hcnt,
-                                                                          d_range);
+        curve_tree_topology<<<(int)((i1 - i0 + 255) / 256), 256, 0, st>>>(T, d_segint, i0, i1, d_height,
+                                                                          d_hcnt + 64 * gi, d_range);
       build_leaves<<<(int)((f1 - f0 + 255) / 256), 256, 0, st>>>(T, d_segall, f0, f1);
       FLN_CUDA(cudaGetLastError());
       launches += 2;
       int32_t hcnt[64];
-      FLN_CUDA(cudaMemcpyAsync(hcnt, d_hcnt, sizeof hcnt, cudaMemcpyDeviceToHost, st));
-      FLN_CUDA(cudaStreamSynchronize(st));
-      int32_t hoff[64];
+      int32_t *hoff = hoff_all.data() + 64 * gi;
       int64_t acc = i0;  // this group's nodes fill bucket[i0, i1)
       for (int h = 0; h < 64; ++h) {
+        hcnt[h] = (int32_t)hc[h];
         hoff[h] = (int32_t)acc;
-        acc += hcnt[h];
+        acc += hc[h];
       }
       if (i1 > i0) {
-        FLN_CUDA(cudaMemcpyAsync(d_hoff, hoff, sizeof hoff, cudaMemcpyHostToDevice, st));
+        FLN_CUDA(cudaMemsetAsync(d_hcur, 0, 64 * sizeof(int32_t), st));
+        FLN_CUDA(cudaMemcpyAsync(d_hoff, hoff, 64 * sizeof(int32_t), cudaMemcpyHostToDevice, st));
         bucket_heights<<<(int)((i1 - i0 + 255) / 256), 256, 0, st>>>(d_height, i0, i1, d_hoff, d_hcur, d_bucket);
         ++launches;
         const int64_t nsmall = (int64_t)hoff[kSmallHeight + 1] - hoff[1];  // heights 1..kSmallHeight
@@ -2791,6 +2830,14 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       }
       k0 = k1;
     }
+    // The device's height counts against the host's, which sized the launches.
+    std::vector<int32_t> dev_counts((size_t)64 * group_end.size());
+    FLN_CUDA(cudaMemcpyAsync(dev_counts.data(), d_hcnt, dev_counts.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             st));
+    FLN_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < dev_counts.size(); ++i)
+      if (dev_counts[i] != host_counts[i])
+        throw Error(FLN_ERR_INTERNAL, "curve-order tree: node heights disagree with their count");
   }
   wait_xyz_pieces(ctx);  // the traversal reads every loop's vertices
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
