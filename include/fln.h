@@ -325,9 +325,11 @@ fln_status fln_learned_gradients(fln_ctx *ctx, const float *params, const float 
  * (fln_params.bh_occupancy) at the best setting; with bit 1 (curve-order
  * trees), then the exact-bucket sizes {4, 6, 10, 12, 16} around it. Beta and the bucket
  * change the real sums within the Barnes-Hut error, never the certificate;
- * the budget changes only their rounding. *out gets *params with the
- * fastest setting; *result the sample times (device time, best of two runs
- * each). */
+ * the budget changes only their rounding. A setting replaces the best so
+ * far only when it is more than 1.5 % faster (timing noise does not choose
+ * between ties). *out gets *params with the fastest setting (its budget
+ * named explicitly); *result the sample times (device time, best of three
+ * runs each). */
 typedef struct fln_tune_result {
   double best_ms;     /* sample time of the chosen setting */
   double default_ms;  /* sample time of *params as given */
