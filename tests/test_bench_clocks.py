@@ -57,3 +57,32 @@ def test_all_samples_when_none_is_inside():
     early = datetime.datetime.now() - datetime.timedelta(seconds=10)
     r = _sampler(mod, [_line(early, 1800)], datetime.datetime.now()).stop()
     assert r["samples_in_timed_region"] == 0 and r["samples"] == 1 and r["sm_mhz"] == 1800.0
+
+
+def test_certificate_text_matches_golden_files():
+    """bench.py compares the CLI's certificate bytes with a text it writes
+    from its own linking numbers: that writer reproduces the committed
+    certificates from their entries (pairs in either order, values off the
+    integer, zeros dropped)."""
+    import glob
+
+    import numpy as np
+
+    mod = _bench()
+    paths = sorted(glob.glob(os.path.join(REPO, "tests", "golden", "certificates", "*.txt")))
+    assert paths
+    rng = np.random.default_rng(5)
+    for p in paths:
+        text = open(p).read()
+        lines = text.strip().splitlines()
+        ncurves = int(lines[0])
+        rows = [tuple(int(x) for x in ln.split(",")) for ln in lines[1:]]
+        pairs = [(j, i) if k % 2 else (i, j) for k, (i, j, _) in enumerate(rows)]
+        lk = [v + rng.uniform(-0.2, 0.2) for (_, _, v) in rows]
+        # Pairs that round to zero are not written.
+        pairs += [(0, 1), (2, 1)]
+        lk += [0.1, -0.2]
+        order = rng.permutation(len(pairs))
+        got = mod.certificate_text(ncurves, np.array(pairs, dtype=np.int64).reshape(-1, 2)[order],
+                                   np.array(lk)[order])
+        assert got == text, p
