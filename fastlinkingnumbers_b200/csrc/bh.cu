@@ -970,7 +970,7 @@ __device__ __noinline__ void shift_down(int2 *stack, int k, int n, int lane) {
 // one per lane (lanes < n), to the warp's
 // open frontier record of `slot`, reserving records as they fill. The open
 // record is (fr, ffill); fr < 0 means none. A record is closed (its header
-// written) when it is full, when the warp moves to another slot, or when the
+// written) when it is full, when the warp moves to another batch, or when the
 // warp finishes.
 __device__ __forceinline__ void front_close(const TravArgs &A, int &fr, int &ffill, int slot, int lane) {
   if (fr >= 0 && lane == 0 && fr < A.front_cap) {
@@ -1126,7 +1126,12 @@ __device__ __forceinline__ void traverse(const TravArgs &A) {
       int frec = s_fstate[w][0], ffill = s_fstate[w][1];
       const int fslot = s_fstate[w][2];
       __syncwarp();
-      if (slot != fslot) front_close(A, frec, ffill, fslot, lane);
+      // Every batch starts its own records: a record then holds the far
+      // pairs of one batch, in that batch's traversal order, whichever warp
+      // ran it and whatever it ran before. (A record shared by consecutive
+      // batches of a slot would group the retry's far-field sums by the
+      // warps' timing, and their last bits with it.)
+      front_close(A, frec, ffill, fslot, lane);
       if (lane == 0) {
         s_fstate[w][0] = frec;
         s_fstate[w][1] = ffill;
@@ -2865,11 +2870,13 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   double *d_counts = ctx.d_bh[13].as<double>(8);  // far, leaf, retried, escalated, status words
   int32_t *d_status = reinterpret_cast<int32_t *>(d_counts + 2);
   // Per slot, fixed point: far-field sum, error estimate, exact sum.
-  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(3 * np + 8);
+  unsigned long long *d_acc = ctx.d_bh[15].as<unsigned long long>(3 * np + 16);
   unsigned long long *d_acc_err = d_acc + np;
   unsigned long long *d_acc_exact = d_acc + 2 * np;
-  // [0] queue, [1] next-round count, [2] exact (or far) chunks, [3] leaf chunks, [4] frontier records
+  // [0] queue, [1] next-round count, [2] exact (or far) chunks, [3] leaf chunks, [4] frontier records;
+  // [8, 12) the copy of [0, 4) for the odd rounds of the fused schedule.
   unsigned long long *d_ctr = d_acc + 3 * np;
+  unsigned long long *const d_ctrs[2] = {d_ctr, d_ctr + 8};
   const TraverseSet &TS = kTraverseSets[prm.bh_occupancy == 6 ? 1 : prm.bh_occupancy == 7 ? 2 : 0];
   static const bool round_log = std::getenv("FLN_BH_ROUND_LOG") != nullptr;
   int per_sm = 64;
@@ -2915,9 +2922,11 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   // batch; a warp writes at most budget + 2 chunks after that.
   const int64_t bkt_soft = int64_t(1) << FLN_BUCKET_SOFT_LOG2;
   const int64_t bkt_cap = bkt_soft + nwarps * (budget + 2);
+  // Two lists: round r writes list r & 1 while the exact-list kernel of
+  // round r - 1 reads the other.
   BucketChunk *d_bkt = nullptr;
   if (prm.bh_schedule == 0)
-    d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)bkt_cap * sizeof(BucketChunk)));
+    d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)(2 * bkt_cap) * sizeof(BucketChunk)));
   if (prm.bh_schedule == 2) {
     d_far = reinterpret_cast<Chunk *>(ctx.d_bh[16].need((size_t)chunk_cap * sizeof(Chunk)));
     d_leaf = reinterpret_cast<Chunk *>(ctx.d_bh[17].need((size_t)chunk_cap * sizeof(Chunk)));
@@ -2963,8 +2972,37 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     if (front) FLN_CUDA(cudaMemsetAsync(d_ctr + 4, 0, sizeof(unsigned long long), st));
     int64_t nin = na, pos = 0;
     int cur = 0;
+    // Fused rounds: round r's exact-list kernel runs on the exact stream
+    // beside round r + 1's traversal. Round r fills list and counters r & 1;
+    // before it clears them it waits for the exact-list kernel of round r - 2
+    // (which read them). Per round three events: the traversal's end (on st),
+    // the exact-list kernel's start and end (on the exact stream).
+    bool pend[2] = {false, false};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    int nev = 0;
+    auto event_at = [&](int x) {
+      while ((int)ctx.ev_round.size() <= x) {
+        cudaEvent_t e = nullptr;
+        FLN_CUDA(cudaEventCreate(&e));
+        ctx.ev_round.push_back(e);
+      }
+      return ctx.ev_round[x];
+    };
+    // The context's stream waits for every exact-list launch of the pass
+    // (also when the pass throws, so that later work stays ordered).
+    auto join = [&]() {
+      if (nev == 0) return;
+      cudaEvent_t e = event_at(3 * nev);
+      FLN_CUDA(cudaEventRecord(e, ctx.exact_stream));
+      FLN_CUDA(cudaStreamWaitEvent(st, e, 0));
+    };
+    if (prm.bh_schedule != 2 && !ctx.exact_stream)
+      FLN_CUDA(cudaStreamCreateWithFlags(&ctx.exact_stream, cudaStreamNonBlocking));
+    try {
     for (int round = 0; (nin > 0 || pos < nstream) && round < 65536; ++round) {
-      FLN_CUDA(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
+      const int par = round & 1;
+      if (prm.bh_schedule != 2 && pend[par]) FLN_CUDA(cudaStreamWaitEvent(st, done[par], 0));
+      FLN_CUDA(cudaMemsetAsync(prm.bh_schedule == 2 ? d_ctr : d_ctrs[par], 0, 4 * sizeof(unsigned long long), st));
       if (prm.bh_schedule == 2) {
         // Classify, then evaluate this round's chunks.
         ClassifyArgs C{d_off, d_base, d_hdr, d_slots, d_itol, prm.epssq, d_batch[cur], nin, d_batch[1 - cur], cap,
@@ -3002,9 +3040,11 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
         continue;
       }
       if (!d_bkt) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut rounds without an exact list");
+      unsigned long long *const c = d_ctrs[par];
+      BucketChunk *const bl = d_bkt + par * bkt_cap;
       TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
-                 d_batch[1 - cur], cap, d_ctr + 1, budget, bucket, d_bkt, d_ctr + 2, bkt_soft, bkt_cap, d_acc,
-                 d_acc_err, d_counts, d_spill, d_ctr, d_status,
+                 d_batch[1 - cur], cap, c + 1, budget, bucket, bl, c + 2, bkt_soft, bkt_cap, d_acc,
+                 d_acc_err, d_counts, d_spill, c, d_status,
                  d_front + pos, nstream - pos, d_skip,
                  front ? d_front : nullptr, d_ctr + 4, front_cap, d_lost, spill_cap,
                  ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
@@ -3026,18 +3066,26 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       else
         (front ? TS.front : cont ? TS.cont : TS.plain)<<<g, 32 * kWarps, 0, st>>>(A);
       FLN_CUDA(cudaGetLastError());
-      BucketArgs BA{d_xyz, d_off, d_slots, d_bkt, d_ctr + 2, bkt_cap, d_acc_exact, d_counts};
-      FLN_CUDA(cudaEventRecord(ctx.ev_bk[0], st));
-      bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, st>>>(BA);
-      FLN_CUDA(cudaGetLastError());
-      FLN_CUDA(cudaEventRecord(ctx.ev_bk[1], st));
+      BucketArgs BA{d_xyz, d_off, d_slots, bl, c + 2, bkt_cap, d_acc_exact, d_counts};
+      {
+        cudaEvent_t et = event_at(3 * nev), e0 = event_at(3 * nev + 1), e1 = event_at(3 * nev + 2);
+        FLN_CUDA(cudaEventRecord(et, st));
+        FLN_CUDA(cudaStreamWaitEvent(ctx.exact_stream, et, 0));
+        FLN_CUDA(cudaEventRecord(e0, ctx.exact_stream));
+        bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, ctx.exact_stream>>>(BA);
+        FLN_CUDA(cudaGetLastError());
+        FLN_CUDA(cudaEventRecord(e1, ctx.exact_stream));
+        done[par] = e1;
+        pend[par] = true;
+        ++nev;
+      }
       launches += 2;
       ++ctx.stats.bh_rounds;
       unsigned long long c2[2];
-      FLN_CUDA(cudaMemcpyAsync(c2, d_ctr, sizeof c2, cudaMemcpyDeviceToHost, st));
+      FLN_CUDA(cudaMemcpyAsync(c2, c, sizeof c2, cudaMemcpyDeviceToHost, st));
       FLN_CUDA(cudaStreamSynchronize(st));
-      ctx.stats.ms_exact += ctx.elapsed(ctx.ev_bk[0], ctx.ev_bk[1]);
       if (round_log) {  // FLN_BH_ROUND_LOG: cumulative counts after each round, for profiling
+        FLN_CUDA(cudaStreamSynchronize(ctx.exact_stream));
         double cnt[8];
         FLN_CUDA(cudaMemcpyAsync(cnt, d_counts, sizeof cnt, cudaMemcpyDeviceToHost, st));
         FLN_CUDA(cudaStreamSynchronize(st));
@@ -3061,6 +3109,12 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       nin = next;
       cur = 1 - cur;
     }
+    } catch (...) {
+      join();
+      throw;
+    }
+    join();
+    for (int x = 0; x < nev; ++x) ctx.stats.ms_exact += ctx.elapsed(ctx.ev_round[3 * x + 1], ctx.ev_round[3 * x + 2]);
     if (nin > 0 || pos < nstream) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut pass did not finish in 65536 rounds");
     if (front) {
       unsigned long long nrec = 0;
@@ -3130,7 +3184,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     // A bounded wait ran out: redo the stage with budgeted rounds, which
     // need the exact list the persistent schedule does not use.
     ctx.stats.bh_wait_timeouts += 1;
-    d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)bkt_cap * sizeof(BucketChunk)));
+    d_bkt = reinterpret_cast<BucketChunk *>(ctx.d_bh[21].need((size_t)(2 * bkt_cap) * sizeof(BucketChunk)));
     d_status = reinterpret_cast<int32_t *>(d_counts + 2);
     FLN_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(double) + sizeof(int32_t), st));
     FLN_CUDA(cudaMemsetAsync(d_counts + 5, 0, 3 * sizeof(double), st));

@@ -31,12 +31,13 @@ Context::Context(int dev, void *user_stream) : device(dev) {
   FLN_CUDA(cudaEventCreate(&ev1));
   FLN_CUDA(cudaEventCreate(&ev2));
   FLN_CUDA(cudaEventCreate(&ev3));
-  for (cudaEvent_t &e : ev_bk) FLN_CUDA(cudaEventCreate(&e));
 }
 
 Context::~Context() {
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
+  if (exact_stream) cudaStreamSynchronize(exact_stream);
+  if (copy_stream) cudaStreamSynchronize(copy_stream);
   for (DevBuf *b : {&d_xyz, &d_off, &d_pairs, &d_loops, &d_items, &d_partial, &d_counter, &d_lk, &d_err, &d_flags,
                     &d_near})
     b->release();
@@ -50,15 +51,13 @@ Context::~Context() {
   if (ev3) cudaEventDestroy(ev3);
   for (cudaEvent_t e : ev_stage)
     if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : ev_bk)
+  if (exact_stream) cudaStreamDestroy(exact_stream);
+  for (cudaEvent_t e : ev_round)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : ev_piece)
     if (e) cudaEventDestroy(e);
   if (ev_before_copy) cudaEventDestroy(ev_before_copy);
-  if (copy_stream) {
-    cudaStreamSynchronize(copy_stream);
-    cudaStreamDestroy(copy_stream);
-  }
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 

@@ -108,7 +108,11 @@ struct Context {
   int64_t bh_front_hint = 0;  // frontier records of the largest Barnes–Hut first pass so far
   HostBuf h_in, h_out;  // pinned staging of copy_h2d / copy_d2h
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
-  cudaEvent_t ev_bk[2] = {nullptr, nullptr};  // around each exact-list launch
+  // The exact-list launches of the fused Barnes–Hut rounds run on their own
+  // stream, beside the next round's traversal; ev_round holds an event pair
+  // around each (grown on demand, kept for later calls).
+  cudaStream_t exact_stream = nullptr;
+  std::vector<cudaEvent_t> ev_round;
   // Vertices from host arrays arrive in pieces on a copy stream (split at
   // loop boundaries); the Barnes–Hut tree build of each piece's loops waits
   // only for its piece. xyz_pieces = 0: the vertices are resident.
