@@ -104,7 +104,7 @@ class ClockSampler:
     the process's own driver calls), and only the samples whose timestamps
     fall between mark() and stop() are kept (all of them if none does)."""
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, interval_ms: int = 200):
         self.path = tempfile.mktemp(suffix=".csv")
         self.t0 = None
         q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -112,7 +112,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", str(interval_ms)],
                                       stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -275,7 +275,7 @@ def run_ours(args, rank, world, local_rank):
                                    d_flags.data_ptr(), method=args.method, params=prm)
         return eng.stats()
 
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(local_rank, args.clock_interval_ms)
     for w in range(args.warmup):
         t0 = time.perf_counter()
         s = step()
@@ -398,6 +398,12 @@ def run_ours(args, rank, world, local_rank):
                   "fp64_recomputed": s_last["fp64_recomputed"], "tree_build_ms": s_last["ms_tree_build"],
                   "far_evals": s_last["bh_far_evals"], "leaf_evals": s_last["bh_leaf_evals"],
                   "nonzero_links": int(np.sum(np.round(lk) != 0)), "flags_recomputed": int(np.sum(flags & 1))},
+        # Each timed step as the library saw it: device time of the call
+        # (events around it), of its Barnes-Hut passes, and host wall time.
+        "timed_steps": {"call_ms": [round(s["ms_kernels"], 2) for s in st],
+                        "passes_ms": [round(s["ms_main_kernel"], 2) for s in st],
+                        "tree_ms": [round(s["ms_tree_build"], 2) for s in st],
+                        "wall_ms": [round(s["ms_total"], 2) for s in st]},
     }
     fx = os.path.join(REPO, "tests", "golden", "configs", args.workload + ".npz")
     if args.method == "barneshut" and os.path.exists(fx) and rank == 0:
@@ -546,6 +552,8 @@ def main():
                          "autotuner's choice)")
     ap.add_argument("--autotune-bucket", type=int, default=1,
                     help="let the autotuner also choose the exact-bucket size (unless --bh-bucket is given)")
+    ap.add_argument("--clock-interval-ms", type=int, default=200,
+                    help="nvidia-smi sampling interval of the clocks record")
     ap.add_argument("--learned-leg", type=int, default=1,
                     help="also train the learned opening criterion on another seed and time one step with it")
     args = ap.parse_args()

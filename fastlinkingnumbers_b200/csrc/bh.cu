@@ -2879,24 +2879,33 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   unsigned long long *const d_ctrs[2] = {d_ctr, d_ctr + 8};
   const TraverseSet &TS = kTraverseSets[prm.bh_occupancy == 6 ? 1 : prm.bh_occupancy == 7 ? 2 : 0];
   static const bool round_log = std::getenv("FLN_BH_ROUND_LOG") != nullptr;
-  int per_sm = 64;
-  for (auto k : {TS.plain, TS.front, TS.cont}) {
-    FLN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, TS.carveout));
-    int n = 0;
-    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * kWarps, 0));
-    per_sm = std::min(per_sm, n);
+  // Carveouts and occupancies are set and queried once per context: driver
+  // queries on every call cost host time while the GPU waits.
+  const int ts_index = (int)(&TS - kTraverseSets);
+  if (ctx.bh_per_sm[ts_index] == 0) {
+    int m = 64;
+    for (auto k : {TS.plain, TS.front, TS.cont}) {
+      FLN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, TS.carveout));
+      int n = 0;
+      FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * kWarps, 0));
+      m = std::min(m, n);
+    }
+    ctx.bh_per_sm[ts_index] = std::max(m, 1);
   }
-  per_sm = std::max(per_sm, 1);
+  if (ctx.bh_per_sm_learned == 0) {
+    int n = 0;
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bh_traverse_learned, 32 * kWarps, 0));
+    ctx.bh_per_sm_learned = std::max(n, 1);
+    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bh_classify, 32 * kWarps, 0));
+    ctx.bh_per_sm_classify = std::max(n, 1);
+  }
+  const int per_sm = ctx.bh_per_sm[ts_index];
   const int grid = ctx.num_sms * per_sm;
   const int grid_f = grid;
   const int64_t nwarps = (int64_t)grid * kWarps;
   const int spill_cap = prm.bh_spill_cap > 0 ? std::min(prm.bh_spill_cap, kSpill) : kSpill;
-  int per_sm_l = 0;
-  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, bh_traverse_learned, 32 * kWarps, 0));
-  const int grid_l = ctx.num_sms * std::max(per_sm_l, 1);  // <= grid: the learned kernel uses more registers
-  int per_sm_c = 0;
-  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, bh_classify, 32 * kWarps, 0));
-  const int grid_c = ctx.num_sms * std::max(per_sm_c, 1);
+  const int grid_l = ctx.num_sms * ctx.bh_per_sm_learned;  // <= grid: the learned kernel uses more registers
+  const int grid_c = ctx.num_sms * ctx.bh_per_sm_classify;
   const int64_t nwarps_c = (int64_t)grid_c * kWarps;
   int2 *d_spill = ctx.d_bh[14].as<int2>((size_t)std::max(nwarps, nwarps_c) * kSpill);
   // Round buffers: a warp hands on at most (kStack + kSpill) / 32 + 1 batches.
@@ -2940,13 +2949,16 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   uint8_t *d_lost = nullptr, *d_skip = nullptr;
   int64_t front_cap = 0;
   if (use_front) {
-    size_t free_b = 0, total_b = 0;
-    FLN_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t have = ctx.d_bh[23].bytes / sizeof(FrontRec);
-    size_t want = ctx.bh_front_hint > 0 ? (size_t)(1.25 * (double)ctx.bh_front_hint) + 1024
-                                        : std::min<size_t>((size_t)16 << 30, free_b / 5) / sizeof(FrontRec);
-    want = std::max(want, have);
-    if (want > have && (want - have) * sizeof(FrontRec) > free_b / 2) want = have + free_b / 2 / sizeof(FrontRec);
+    const size_t want_hint = ctx.bh_front_hint > 0 ? (size_t)(1.25 * (double)ctx.bh_front_hint) + 1024 : 0;
+    size_t want = have;
+    if (want_hint == 0 || want_hint > have) {  // the buffer must grow: ask how much memory is free
+      size_t free_b = 0, total_b = 0;
+      FLN_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      want = want_hint > 0 ? want_hint : std::min<size_t>((size_t)16 << 30, free_b / 5) / sizeof(FrontRec);
+      want = std::max(want, have);
+      if (want > have && (want - have) * sizeof(FrontRec) > free_b / 2) want = have + free_b / 2 / sizeof(FrontRec);
+    }
     front_cap = (int64_t)std::max<size_t>(want, 1024);
     d_front = reinterpret_cast<FrontRec *>(ctx.d_bh[23].need((size_t)front_cap * sizeof(FrontRec)));
     d_lost = ctx.d_bh[25].as<uint8_t>(2 * np);

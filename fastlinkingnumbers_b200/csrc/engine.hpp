@@ -106,6 +106,10 @@ struct Context {
   DevBuf d_xyz, d_off, d_pairs, d_loops, d_items, d_partial, d_counter, d_lk, d_err, d_flags, d_near;
   DevBuf d_bh[28];
   int64_t bh_front_hint = 0;  // frontier records of the largest Barnes–Hut first pass so far
+  // CTAs per SM of the traversal kernels (per occupancy set), of the learned
+  // traversal and of bh_classify; 0 until first queried.
+  int bh_per_sm[3] = {0, 0, 0};
+  int bh_per_sm_learned = 0, bh_per_sm_classify = 0;
   HostBuf h_in, h_out;  // pinned staging of copy_h2d / copy_d2h
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   // The exact-list launches of the fused Barnes–Hut rounds run on their own
