@@ -3168,9 +3168,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
                   prm.bh_err_limit, prm.bh_escalations, d_sitol, d_pass_arr, d_left, d_acc, d_acc_err, d_ring,
                   d_ready, d_q, d_lk_out, d_err_out, d_fl, d_cnt4, d_spill, d_status, spill_cap,
                   prm.bh_wait_polls > 0 ? (long long)prm.bh_wait_polls : kWaitPolls};
-    int per_sm_p = 0;
-    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, bh_persistent, 32 * kWarps, 0));
-    const int gp = std::min(grid, ctx.num_sms * std::max(per_sm_p, 1));
+    const int gp = std::min(grid, ctx.num_sms * occupancy_of((const void *)bh_persistent, 32 * kWarps));
     FLN_CUDA(cudaEventRecord(ctx.ev2, st));
     bh_persistent<<<gp, 32 * kWarps, 0, st>>>(P);
     FLN_CUDA(cudaGetLastError());

@@ -421,14 +421,13 @@ static_assert(kShapes[0].block == kBlockSegs && kShapes[0].tile == kTile, "the d
 
 template <int kB, int kT>
 void launch_direct_t(cudaStream_t st, int sms, int precision, const DirectArgs &A) {
-  int per_sm = 0;
   if (precision == FLN_PREC_FP64) {
-    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel<kB, kT>, kB, 0));
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.items, (int64_t)sms * std::max(per_sm, 1)));
+    const int per_sm = occupancy_of((const void *)direct_fp64_kernel<kB, kT>, kB);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.items, (int64_t)sms * per_sm));
     direct_fp64_kernel<kB, kT><<<grid, kB, 0, st>>>(A);
   } else {
-    FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel<kB, kT>, kB, 0));
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.items, (int64_t)sms * std::max(per_sm, 1)));
+    const int per_sm = occupancy_of((const void *)direct_mixed_kernel<kB, kT>, kB);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.items, (int64_t)sms * per_sm));
     direct_mixed_kernel<kB, kT><<<grid, kB, 0, st>>>(A);
   }
 }
@@ -703,11 +702,11 @@ extern "C" fln_status fln_linking_numbers_direct_noalloc(const double *d_xyz, co
                reinterpret_cast<double *>(scratch + kNaPartial), reinterpret_cast<unsigned long long *>(scratch),
                (float)kDefaultNearFactor};
   if (precision == FLN_PREC_FP64) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_fp64_kernel<kBlockSegs, kTile>, kBlockSegs, 0);
+    per_sm = occupancy_of((const void *)direct_fp64_kernel<kBlockSegs, kTile>, kBlockSegs);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));
     direct_fp64_kernel<kBlockSegs, kTile><<<grid, kBlockSegs, 0, s>>>(A);
   } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, direct_mixed_kernel<kBlockSegs, kTile>, kBlockSegs, 0);
+    per_sm = occupancy_of((const void *)direct_mixed_kernel<kBlockSegs, kTile>, kBlockSegs);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h.total_items, (int64_t)sms * std::max(per_sm, 1)));
     direct_mixed_kernel<kBlockSegs, kTile><<<grid, kBlockSegs, 0, s>>>(A);
   }

@@ -733,9 +733,7 @@ void discretize_device(Context &ctx, const std::vector<CurveData> &curves, const
     std::memcpy(&v, &md, sizeof v);
     return v;
   };
-  int per_sm = 0;
-  FLN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, disc_traverse, 32 * kDWarps, 0));
-  const int grid = ctx.num_sms * std::max(per_sm, 1);
+  const int grid = ctx.num_sms * occupancy_of((const void *)disc_traverse, 32 * kDWarps);
   const int64_t nwarps = (int64_t)grid * kDWarps;
   int64_t out_cap = 0;
   for (int it = 0; it < kMaxRounds; ++it) {

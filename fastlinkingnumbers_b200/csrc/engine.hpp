@@ -4,7 +4,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -149,6 +153,25 @@ struct Context {
 inline void wait_xyz_pieces(Context &c) {
   for (int i = 0; i < c.xyz_pieces; ++i) cudaStreamWaitEvent(c.stream, c.ev_piece[i], 0);
   c.xyz_pieces = 0;
+}
+
+// Resident CTAs per SM of `kernel` at `block` threads (at least 1), asked of
+// the driver once per kernel and block size: the library is built for one
+// architecture, and a driver query on every call costs host time while the
+// GPU waits.
+inline int occupancy_of(const void *kernel, int block) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kernel, block);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  return cache[key] = std::max(n, 1);
 }
 
 // Mixed direct sum: a segment pair whose closest endpoint distance is below
