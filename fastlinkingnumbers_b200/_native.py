@@ -86,7 +86,8 @@ class Stats(C.Structure):
         ("bh_escalated", C.c_int64), ("bh_wait_timeouts", C.c_int64),
         ("ms_exact", C.c_double), ("bh_exact_entries", C.c_double), ("ms_retry", C.c_double),
         ("bh_front_records", C.c_int64), ("bh_retry_from_roots", C.c_int64),
-        ("bh_far_reused", C.c_double), ("bh_far_subtracted", C.c_double), ("reserved_stats2", C.c_double * 2),
+        ("bh_far_reused", C.c_double), ("bh_far_subtracted", C.c_double), ("ms_traverse", C.c_double),
+        ("reserved_stats2", C.c_double * 1),
     ]
 
     def as_dict(self):

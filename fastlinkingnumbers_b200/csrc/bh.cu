@@ -2987,8 +2987,9 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     // Fused rounds: round r's exact-list kernel runs on the exact stream
     // beside round r + 1's traversal. Round r fills list and counters r & 1;
     // before it clears them it waits for the exact-list kernel of round r - 2
-    // (which read them). Per round three events: the traversal's end (on st),
-    // the exact-list kernel's start and end (on the exact stream).
+    // (which read them). Per round four events: the traversal's end (on st),
+    // the exact-list kernel's start and end (on the exact stream), the
+    // traversal's start (on st).
     bool pend[2] = {false, false};
     cudaEvent_t done[2] = {nullptr, nullptr};
     int nev = 0;
@@ -3004,7 +3005,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     // (also when the pass throws, so that later work stays ordered).
     auto join = [&]() {
       if (nev == 0) return;
-      cudaEvent_t e = event_at(3 * nev);
+      cudaEvent_t e = event_at(4 * nev);
       FLN_CUDA(cudaEventRecord(e, ctx.exact_stream));
       FLN_CUDA(cudaStreamWaitEvent(st, e, 0));
     };
@@ -3070,6 +3071,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       const int gmax = (A.learned.frag && !A.rec) ? grid_l : (front ? grid_f : grid);
       const int64_t work = nin + (nstream - pos);
       const int g = (int)std::max<int64_t>(1, std::min<int64_t>((work + kWarps - 1) / kWarps, gmax));
+      FLN_CUDA(cudaEventRecord(event_at(4 * nev + 3), st));
       if (A.rec)
         bh_traverse_record<<<g, 32 * kWarps, 0, st>>>(A);
       else if (A.learned.frag)
@@ -3080,7 +3082,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       FLN_CUDA(cudaGetLastError());
       BucketArgs BA{d_xyz, d_off, d_slots, bl, c + 2, bkt_cap, d_acc_exact, d_counts};
       {
-        cudaEvent_t et = event_at(3 * nev), e0 = event_at(3 * nev + 1), e1 = event_at(3 * nev + 2);
+        cudaEvent_t et = event_at(4 * nev), e0 = event_at(4 * nev + 1), e1 = event_at(4 * nev + 2);
         FLN_CUDA(cudaEventRecord(et, st));
         FLN_CUDA(cudaStreamWaitEvent(ctx.exact_stream, et, 0));
         FLN_CUDA(cudaEventRecord(e0, ctx.exact_stream));
@@ -3126,7 +3128,10 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       throw;
     }
     join();
-    for (int x = 0; x < nev; ++x) ctx.stats.ms_exact += ctx.elapsed(ctx.ev_round[3 * x + 1], ctx.ev_round[3 * x + 2]);
+    for (int x = 0; x < nev; ++x) {
+      ctx.stats.ms_exact += ctx.elapsed(ctx.ev_round[4 * x + 1], ctx.ev_round[4 * x + 2]);
+      ctx.stats.ms_traverse += ctx.elapsed(ctx.ev_round[4 * x + 3], ctx.ev_round[4 * x]);
+    }
     if (nin > 0 || pos < nstream) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut pass did not finish in 65536 rounds");
     if (front) {
       unsigned long long nrec = 0;

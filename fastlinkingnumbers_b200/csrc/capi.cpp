@@ -147,7 +147,7 @@ static int run_pairs(Context &ctx, const double *d_xyz, const int64_t *d_off, co
   ctx.stats.ms_main_kernel = 0;
   ctx.stats.ms_tree_build = 0;
   ctx.stats.bh_far_evals = ctx.stats.bh_leaf_evals = 0;
-  ctx.stats.ms_exact = ctx.stats.bh_exact_entries = 0;
+  ctx.stats.ms_exact = ctx.stats.bh_exact_entries = ctx.stats.ms_traverse = 0;
   ctx.stats.ms_retry = 0;
   ctx.stats.bh_front_records = ctx.stats.bh_retry_from_roots = 0;
   ctx.stats.bh_wait_timeouts = 0;

@@ -153,7 +153,11 @@ typedef struct fln_stats {
                                    first-pass values were kept (not evaluated again) */
   double bh_far_subtracted;     /* Barnes–Hut: frontier node pairs opened by the retry, whose first-pass
                                    values were given back */
-  double reserved_stats2[2];
+  double ms_traverse;           /* Barnes–Hut bh_schedule 0: device time of the traversal launches (CUDA
+                                   events on the launching stream; the exact-list launches run beside them
+                                   on a second stream, so ms_traverse + ms_exact can exceed
+                                   ms_main_kernel) */
+  double reserved_stats2[1];
 } fln_stats;
 
 typedef struct fln_ctx fln_ctx;
