@@ -171,7 +171,10 @@ void fln_default_params(fln_params *p);
 
 /* Context: one CUDA device and one stream; owns all device buffers.
  * stream = 0 creates a private stream; otherwise the given cudaStream_t
- * (as an opaque pointer) is used and not destroyed. */
+ * (as an opaque pointer) is used and not destroyed. The context also keeps
+ * two internal streams (the pieces of a pinned vertex copy; the Barnes-Hut
+ * exact-list launches), joined back to `stream` by events before a call's
+ * results are read, so work queued on `stream` after a call sees them. */
 fln_status fln_ctx_create(int device, void *stream, fln_ctx **out);
 void fln_ctx_destroy(fln_ctx *ctx);
 fln_status fln_ctx_stats(const fln_ctx *ctx, fln_stats *out);
