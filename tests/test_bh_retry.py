@@ -104,6 +104,24 @@ def test_continued_retry_equals_retry_from_roots(engine, case):
           f"(from roots {s_r['ms_retry']:.2f} ms), far {s_c['bh_far_evals']:.3g} vs {s_r['bh_far_evals']:.3g}")
 
 
+@pytest.mark.parametrize("budget", [0, 16])
+def test_repeated_calls_are_bit_identical(engine, budget):
+    # Each batch writes its own frontier records and exact-list chunks and
+    # adds its far-field sum once, so a slot's sums are the same integer sums
+    # of the same partial sums in every call, whatever the warps' timing (the
+    # exact list also runs beside the next traversal on a second stream). A
+    # small budget spreads each loop pair over many batches.
+    poff, pxyz, pairs = _polymer(engine, seed=61, loops=30, cube=250.0)
+    runs = []
+    for _ in range(3):
+        runs.append(engine.linking_numbers(pxyz, poff, pairs, "barneshut", bh_budget=budget))
+        s = engine.stats()
+        assert s["beta_retried"] > 0 and s["bh_front_records"] > 0 and s["bh_retry_from_roots"] == 0
+    for lk, err, fl in runs[1:]:
+        assert np.array_equal(lk, runs[0][0]) and np.array_equal(err, runs[0][1])
+        np.testing.assert_array_equal(fl, runs[0][2])
+
+
 def test_learned_criterion_with_continued_retry(engine):
     # The learned criterion scales its threshold with (beta0 / beta)^4, so a
     # pair it opens at beta0 it also opens at beta*: the continuation applies.
