@@ -306,6 +306,18 @@ def run_ours(args, rank, world, local_rank):
     lk = d_lk.cpu().numpy()
     flags = d_flags.cpu().numpy()
     value = world * units / (ms * 1e-3) / 1e9
+    # One untimed step with each round's exact list after its traversal on one
+    # stream (bh_exact_serial; the same results bit for bit): each kernel's
+    # own CUDA-event time, which the overlapped timed steps cannot give.
+    alone = None
+    if args.method == "barneshut" and args.bh_schedule == 0:
+        prm_serial = type(prm).from_buffer_copy(prm)
+        prm_serial.bh_exact_serial = 1
+        eng.linking_numbers_device(d_xyz.data_ptr(), d_off.data_ptr(), len(poff) - 1, d_pairs.data_ptr(), npairs,
+                                   d_lk.data_ptr(), d_err.data_ptr(), d_flags.data_ptr(), method=args.method,
+                                   params=prm_serial)
+        alone = eng.stats()
+        assert np.array_equal(d_lk.cpu().numpy(), lk), "the serial exact list changed the sums"
 
     # End to end through the host-array entry point: H2D of the polylines and
     # pairs, the whole stage, D2H of the per-pair results, every step.
@@ -357,6 +369,14 @@ def run_ours(args, rank, world, local_rank):
                 "dram_gbs": dram_gbs, "dram_frac": dram_gbs / peaks["hbm_gbs"] if dram_gbs else None,
                 "limiter": "L1 wavefronts and dependent-load latency (node records are re-read from L1/L2); "
                            "DRAM runs at dram_frac of the copy peak",
+                "alone": None if alone is None else {
+                    "note": "one untimed step with each exact list after its traversal on one stream",
+                    "traversal_ms": alone["ms_traverse"],
+                    "achieved": alg / (alone["ms_traverse"] * 1e-3) / 1e9,
+                    "frac": alg / (alone["ms_traverse"] * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                    "exact_ms": alone["ms_exact"],
+                    "exact_Gsegpair_per_s": seg_exact / (alone["ms_exact"] * 1e-3) / 1e9,
+                    "passes_ms": alone["ms_main_kernel"]},
                 "exact_kernel": {"kernel": "bh_buckets", "ms_per_step": exact_ms,
                                  "segment_pairs_per_step": seg_exact,
                                  "Gsegpair_per_s": seg_exact / (exact_ms * 1e-3) / 1e9 if exact_ms > 0 else None,
@@ -369,8 +389,11 @@ def run_ours(args, rank, world, local_rank):
                          "bytes = 2 x 184 B FP32 node record per far-field node pair + 2 x 32 B (centre, "
                          "radius) per node pair handed to the exact list; traffic = DRAM read+write per "
                          "node pair from the small-case ncu captures in "
-                         "profiles/bh_traverse_bh_buckets_polymer_6M.md x node pairs; node records are mostly re-read from L1/L2: the kernel is bound by "
-                         "L1 wavefronts and latency, not by HBM")}
+                         "profiles/bh_traverse_bh_buckets_polymer_6M.md x node pairs; node records are "
+                         "mostly re-read from L1/L2: the kernel is bound by L1 wavefronts and latency, not "
+                         "by HBM. In the timed steps each round's exact list runs beside the next "
+                         "traversal on a second stream, so a traversal launch's events include the time "
+                         "the two kernels share the SMs; 'alone' times them one after the other")}
     else:
         roof = {"bound": "fp32-issue", "kernel": "direct_" + args.precision, "ms_per_launch": main_ms,
                 "segment_pairs_per_s": units / (main_ms * 1e-3)}

@@ -70,7 +70,7 @@ class Params(C.Structure):
         ("bh_schedule", C.c_int32), ("host_prepare", C.c_int32), ("bh_budget", C.c_int32),
         ("bh_bucket", C.c_int32), ("bh_retry_from_roots", C.c_int32), ("bh_spill_cap", C.c_int32),
         ("bh_wait_polls", C.c_int64), ("direct_tile", C.c_int32), ("bh_occupancy", C.c_int32),
-        ("reserved_params", C.c_double * 4),
+        ("bh_exact_serial", C.c_int32), ("reserved_int", C.c_int32), ("reserved_params", C.c_double * 3),
     ]
 
 

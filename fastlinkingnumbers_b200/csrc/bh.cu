@@ -3082,13 +3082,15 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       FLN_CUDA(cudaGetLastError());
       BucketArgs BA{d_xyz, d_off, d_slots, bl, c + 2, bkt_cap, d_acc_exact, d_counts};
       {
+        // bh_exact_serial: on the context's stream, after its traversal.
+        cudaStream_t xs = prm.bh_exact_serial ? st : ctx.exact_stream;
         cudaEvent_t et = event_at(4 * nev), e0 = event_at(4 * nev + 1), e1 = event_at(4 * nev + 2);
         FLN_CUDA(cudaEventRecord(et, st));
-        FLN_CUDA(cudaStreamWaitEvent(ctx.exact_stream, et, 0));
-        FLN_CUDA(cudaEventRecord(e0, ctx.exact_stream));
-        bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, ctx.exact_stream>>>(BA);
+        FLN_CUDA(cudaStreamWaitEvent(xs, et, 0));
+        FLN_CUDA(cudaEventRecord(e0, xs));
+        bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, xs>>>(BA);
         FLN_CUDA(cudaGetLastError());
-        FLN_CUDA(cudaEventRecord(e1, ctx.exact_stream));
+        FLN_CUDA(cudaEventRecord(e1, xs));
         done[par] = e1;
         pend[par] = true;
         ++nev;

@@ -114,7 +114,12 @@ typedef struct fln_params {
   int32_t bh_occupancy;         /* CTAs per SM of the Barnes-Hut traversal kernels: 0 = 5 (96 registers),
                                    5, 6 (80 registers) or 7 (72, some spills); more resident warps hide more of
                                    the traversal's dependent loads. Chosen by fln_autotune; results do not change */
-  double reserved_params[4];    /* zero */
+  int32_t bh_exact_serial;      /* bh_schedule 0: 0 = each round's exact list runs on a second stream beside
+                                   the next round's traversal (default); 1 = on the context's stream after
+                                   its traversal, so that each kernel's CUDA-event time is its own (for
+                                   measuring; results are the same bit for bit) */
+  int32_t reserved_int;         /* zero */
+  double reserved_params[3];    /* zero */
 } fln_params;
 
 /* Statistics of the last computation on a context. */

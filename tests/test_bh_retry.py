@@ -122,6 +122,20 @@ def test_repeated_calls_are_bit_identical(engine, budget):
         np.testing.assert_array_equal(fl, runs[0][2])
 
 
+def test_serial_exact_list_gives_the_same_bits(engine):
+    # bh_exact_serial runs each round's exact list on the context's stream
+    # after its traversal instead of beside the next one: the same work, the
+    # same partial sums, so the same bits.
+    poff, pxyz, pairs = _polymer(engine, seed=61, loops=30, cube=250.0)
+    a = engine.linking_numbers(pxyz, poff, pairs, "barneshut")
+    s_a = engine.stats()
+    b = engine.linking_numbers(pxyz, poff, pairs, "barneshut", bh_exact_serial=1)
+    s_b = engine.stats()
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert s_a["ms_traverse"] > 0 and s_b["ms_traverse"] > 0 and s_a["ms_exact"] > 0 and s_b["ms_exact"] > 0
+
+
 def test_learned_criterion_with_continued_retry(engine):
     # The learned criterion scales its threshold with (beta0 / beta)^4, so a
     # pair it opens at beta0 it also opens at beta*: the continuation applies.
