@@ -3012,119 +3012,120 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     if (prm.bh_schedule != 2 && !ctx.exact_stream)
       FLN_CUDA(cudaStreamCreateWithFlags(&ctx.exact_stream, cudaStreamNonBlocking));
     try {
-    for (int round = 0; (nin > 0 || pos < nstream) && round < 65536; ++round) {
-      const int par = round & 1;
-      if (prm.bh_schedule != 2 && pend[par]) FLN_CUDA(cudaStreamWaitEvent(st, done[par], 0));
-      FLN_CUDA(cudaMemsetAsync(prm.bh_schedule == 2 ? d_ctr : d_ctrs[par], 0, 4 * sizeof(unsigned long long), st));
-      if (prm.bh_schedule == 2) {
-        // Classify, then evaluate this round's chunks.
-        ClassifyArgs C{d_off, d_base, d_hdr, d_slots, d_itol, prm.epssq, d_batch[cur], nin, d_batch[1 - cur], cap,
-                       d_ctr + 1, budget, d_far, d_leaf, d_ctr + 2, d_ctr + 3, chunk_soft, chunk_cap, d_spill,
-                       d_ctr, d_status};
-        const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, grid_c));
-        bh_classify<<<g, 32 * kWarps, 0, st>>>(C);
+      for (int round = 0; (nin > 0 || pos < nstream) && round < 65536; ++round) {
+        const int par = round & 1;
+        if (prm.bh_schedule != 2 && pend[par]) FLN_CUDA(cudaStreamWaitEvent(st, done[par], 0));
+        FLN_CUDA(cudaMemsetAsync(prm.bh_schedule == 2 ? d_ctr : d_ctrs[par], 0, 4 * sizeof(unsigned long long), st));
+        if (prm.bh_schedule == 2) {
+          // Classify, then evaluate this round's chunks.
+          ClassifyArgs C{d_off, d_base, d_hdr, d_slots, d_itol, prm.epssq, d_batch[cur], nin, d_batch[1 - cur], cap,
+                         d_ctr + 1, budget, d_far, d_leaf, d_ctr + 2, d_ctr + 3, chunk_soft, chunk_cap, d_spill,
+                         d_ctr, d_status};
+          const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nin + kWarps - 1) / kWarps, grid_c));
+          bh_classify<<<g, 32 * kWarps, 0, st>>>(C);
+          FLN_CUDA(cudaGetLastError());
+          unsigned long long c4[4];
+          FLN_CUDA(cudaMemcpyAsync(c4, d_ctr, sizeof c4, cudaMemcpyDeviceToHost, st));
+          FLN_CUDA(cudaStreamSynchronize(st));
+          const int64_t nfar = (int64_t)std::min<unsigned long long>(c4[2], (unsigned long long)chunk_cap);
+          const int64_t nleaf = (int64_t)std::min<unsigned long long>(c4[3], (unsigned long long)chunk_cap);
+          EvalArgs E{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, prm.epssq, d_far, nfar, d_acc, d_acc_err, d_counts};
+          if (nfar > 0) bh_far_chunks<<<(int)((nfar * 32 + 255) / 256), 256, 0, st>>>(E);
+          E.chunks = d_leaf;
+          E.nchunks = nleaf;
+          E.count = d_counts + 1;
+          if (nleaf > 0) bh_leaf_chunks<<<(int)((nleaf * 32 + 255) / 256), 256, 0, st>>>(E);
+          FLN_CUDA(cudaGetLastError());
+          launches += 3;
+          ++ctx.stats.bh_rounds;
+          // Batches not taken this round (past the chunk soft limit) carry over.
+          int64_t next = (int64_t)std::min<unsigned long long>(c4[1], (unsigned long long)cap);
+          const int64_t taken = (int64_t)std::min<unsigned long long>(c4[0], (unsigned long long)nin);
+          if (taken < nin) {
+            const int64_t keep = std::min<int64_t>(nin - taken, cap - next);
+            FLN_CUDA(cudaMemcpyAsync(d_batch[1 - cur] + next, d_batch[cur] + taken, keep * sizeof(Batch),
+                                     cudaMemcpyDeviceToDevice, st));
+            if (keep < nin - taken) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut round buffer too small");
+            next += keep;
+          }
+          nin = next;
+          cur = 1 - cur;
+          continue;
+        }
+        if (!d_bkt) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut rounds without an exact list");
+        unsigned long long *const c = d_ctrs[par];
+        BucketChunk *const bl = d_bkt + par * bkt_cap;
+        TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
+                   d_batch[1 - cur], cap, c + 1, budget, bucket, bl, c + 2, bkt_soft, bkt_cap, d_acc,
+                   d_acc_err, d_counts, d_spill, c, d_status,
+                   d_front + pos, nstream - pos, d_skip,
+                   front ? d_front : nullptr, d_ctr + 4, front_cap, d_lost, spill_cap,
+                   ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
+        if (record) {
+          A.rec = ctx.recording.rec;
+          A.rec_count = ctx.recording.count;
+          A.rec_cap = ctx.recording.cap;
+          A.rec_smin = ctx.recording.s_min;
+          A.rec_keep = ctx.recording.keep;
+        }
+        const int gmax = (A.learned.frag && !A.rec) ? grid_l : (front ? grid_f : grid);
+        const int64_t work = nin + (nstream - pos);
+        const int g = (int)std::max<int64_t>(1, std::min<int64_t>((work + kWarps - 1) / kWarps, gmax));
+        FLN_CUDA(cudaEventRecord(event_at(4 * nev + 3), st));
+        if (A.rec)
+          bh_traverse_record<<<g, 32 * kWarps, 0, st>>>(A);
+        else if (A.learned.frag)
+          (front ? bh_traverse_learned_front : cont ? bh_traverse_learned_cont : bh_traverse_learned)
+              <<<g, 32 * kWarps, 0, st>>>(A);
+        else
+          (front ? TS.front : cont ? TS.cont : TS.plain)<<<g, 32 * kWarps, 0, st>>>(A);
         FLN_CUDA(cudaGetLastError());
-        unsigned long long c4[4];
-        FLN_CUDA(cudaMemcpyAsync(c4, d_ctr, sizeof c4, cudaMemcpyDeviceToHost, st));
-        FLN_CUDA(cudaStreamSynchronize(st));
-        const int64_t nfar = (int64_t)std::min<unsigned long long>(c4[2], (unsigned long long)chunk_cap);
-        const int64_t nleaf = (int64_t)std::min<unsigned long long>(c4[3], (unsigned long long)chunk_cap);
-        EvalArgs E{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, prm.epssq, d_far, nfar, d_acc, d_acc_err, d_counts};
-        if (nfar > 0) bh_far_chunks<<<(int)((nfar * 32 + 255) / 256), 256, 0, st>>>(E);
-        E.chunks = d_leaf;
-        E.nchunks = nleaf;
-        E.count = d_counts + 1;
-        if (nleaf > 0) bh_leaf_chunks<<<(int)((nleaf * 32 + 255) / 256), 256, 0, st>>>(E);
-        FLN_CUDA(cudaGetLastError());
-        launches += 3;
+        BucketArgs BA{d_xyz, d_off, d_slots, bl, c + 2, bkt_cap, d_acc_exact, d_counts};
+        {
+          // bh_exact_serial: on the context's stream, after its traversal.
+          cudaStream_t xs = prm.bh_exact_serial ? st : ctx.exact_stream;
+          cudaEvent_t et = event_at(4 * nev), e0 = event_at(4 * nev + 1), e1 = event_at(4 * nev + 2);
+          FLN_CUDA(cudaEventRecord(et, st));
+          FLN_CUDA(cudaStreamWaitEvent(xs, et, 0));
+          FLN_CUDA(cudaEventRecord(e0, xs));
+          bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, xs>>>(BA);
+          FLN_CUDA(cudaGetLastError());
+          FLN_CUDA(cudaEventRecord(e1, xs));
+          done[par] = e1;
+          pend[par] = true;
+          ++nev;
+        }
+        launches += 2;
         ++ctx.stats.bh_rounds;
-        // Batches not taken this round (past the chunk soft limit) carry over.
-        int64_t next = (int64_t)std::min<unsigned long long>(c4[1], (unsigned long long)cap);
-        const int64_t taken = (int64_t)std::min<unsigned long long>(c4[0], (unsigned long long)nin);
+        unsigned long long c2[2];
+        FLN_CUDA(cudaMemcpyAsync(c2, c, sizeof c2, cudaMemcpyDeviceToHost, st));
+        FLN_CUDA(cudaStreamSynchronize(st));
+        if (round_log) {  // FLN_BH_ROUND_LOG: cumulative counts after each round, for profiling
+          FLN_CUDA(cudaStreamSynchronize(ctx.exact_stream));
+          double cnt[8];
+          FLN_CUDA(cudaMemcpyAsync(cnt, d_counts, sizeof cnt, cudaMemcpyDeviceToHost, st));
+          FLN_CUDA(cudaStreamSynchronize(st));
+          std::fprintf(stderr,
+                       "[fln] round %d (%s): far node pairs %.0f, exact node pairs %.0f, exact segment pairs %.0f\n",
+                       ctx.stats.bh_rounds, front ? "first pass" : cont ? "continued retry" : "from roots", cnt[0],
+                       cnt[5], cnt[1]);
+        }
+        // Input not taken this round (past the soft limit) carries over: the
+        // batches by copy, the frontier records by position.
+        int64_t next = (int64_t)std::min<unsigned long long>(c2[1], (unsigned long long)cap);
+        const int64_t taken = (int64_t)std::min<unsigned long long>(c2[0], (unsigned long long)(nin + nstream - pos));
         if (taken < nin) {
           const int64_t keep = std::min<int64_t>(nin - taken, cap - next);
           FLN_CUDA(cudaMemcpyAsync(d_batch[1 - cur] + next, d_batch[cur] + taken, keep * sizeof(Batch),
                                    cudaMemcpyDeviceToDevice, st));
           if (keep < nin - taken) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut round buffer too small");
           next += keep;
+        } else {
+          pos += taken - nin;
         }
         nin = next;
         cur = 1 - cur;
-        continue;
       }
-      if (!d_bkt) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut rounds without an exact list");
-      unsigned long long *const c = d_ctrs[par];
-      BucketChunk *const bl = d_bkt + par * bkt_cap;
-      TravArgs A{d_xyz, d_off, d_base, d_hdr, d_mom, d_slots, d_itol, prm.epssq, d_batch[cur], nin,
-                 d_batch[1 - cur], cap, c + 1, budget, bucket, bl, c + 2, bkt_soft, bkt_cap, d_acc,
-                 d_acc_err, d_counts, d_spill, c, d_status,
-                 d_front + pos, nstream - pos, d_skip,
-                 front ? d_front : nullptr, d_ctr + 4, front_cap, d_lost, spill_cap,
-                 ctx.learned, b0, nullptr, nullptr, 0, 0.f, 0u};
-      if (record) {
-        A.rec = ctx.recording.rec;
-        A.rec_count = ctx.recording.count;
-        A.rec_cap = ctx.recording.cap;
-        A.rec_smin = ctx.recording.s_min;
-        A.rec_keep = ctx.recording.keep;
-      }
-      const int gmax = (A.learned.frag && !A.rec) ? grid_l : (front ? grid_f : grid);
-      const int64_t work = nin + (nstream - pos);
-      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((work + kWarps - 1) / kWarps, gmax));
-      FLN_CUDA(cudaEventRecord(event_at(4 * nev + 3), st));
-      if (A.rec)
-        bh_traverse_record<<<g, 32 * kWarps, 0, st>>>(A);
-      else if (A.learned.frag)
-        (front ? bh_traverse_learned_front : cont ? bh_traverse_learned_cont : bh_traverse_learned)
-            <<<g, 32 * kWarps, 0, st>>>(A);
-      else
-        (front ? TS.front : cont ? TS.cont : TS.plain)<<<g, 32 * kWarps, 0, st>>>(A);
-      FLN_CUDA(cudaGetLastError());
-      BucketArgs BA{d_xyz, d_off, d_slots, bl, c + 2, bkt_cap, d_acc_exact, d_counts};
-      {
-        // bh_exact_serial: on the context's stream, after its traversal.
-        cudaStream_t xs = prm.bh_exact_serial ? st : ctx.exact_stream;
-        cudaEvent_t et = event_at(4 * nev), e0 = event_at(4 * nev + 1), e1 = event_at(4 * nev + 2);
-        FLN_CUDA(cudaEventRecord(et, st));
-        FLN_CUDA(cudaStreamWaitEvent(xs, et, 0));
-        FLN_CUDA(cudaEventRecord(e0, xs));
-        bh_buckets<<<ctx.num_sms * 2 * FLN_BUCKET_MIN_CTAS, 32 * kBkWarps, 0, xs>>>(BA);
-        FLN_CUDA(cudaGetLastError());
-        FLN_CUDA(cudaEventRecord(e1, xs));
-        done[par] = e1;
-        pend[par] = true;
-        ++nev;
-      }
-      launches += 2;
-      ++ctx.stats.bh_rounds;
-      unsigned long long c2[2];
-      FLN_CUDA(cudaMemcpyAsync(c2, c, sizeof c2, cudaMemcpyDeviceToHost, st));
-      FLN_CUDA(cudaStreamSynchronize(st));
-      if (round_log) {  // FLN_BH_ROUND_LOG: cumulative counts after each round, for profiling
-        FLN_CUDA(cudaStreamSynchronize(ctx.exact_stream));
-        double cnt[8];
-        FLN_CUDA(cudaMemcpyAsync(cnt, d_counts, sizeof cnt, cudaMemcpyDeviceToHost, st));
-        FLN_CUDA(cudaStreamSynchronize(st));
-        std::fprintf(stderr, "[fln] round %d (%s): far node pairs %.0f, exact node pairs %.0f, exact segment pairs %.0f\n",
-                     ctx.stats.bh_rounds, front ? "first pass" : cont ? "continued retry" : "from roots", cnt[0],
-                     cnt[5], cnt[1]);
-      }
-      // Input not taken this round (past the soft limit) carries over: the
-      // batches by copy, the frontier records by position.
-      int64_t next = (int64_t)std::min<unsigned long long>(c2[1], (unsigned long long)cap);
-      const int64_t taken = (int64_t)std::min<unsigned long long>(c2[0], (unsigned long long)(nin + nstream - pos));
-      if (taken < nin) {
-        const int64_t keep = std::min<int64_t>(nin - taken, cap - next);
-        FLN_CUDA(cudaMemcpyAsync(d_batch[1 - cur] + next, d_batch[cur] + taken, keep * sizeof(Batch),
-                                 cudaMemcpyDeviceToDevice, st));
-        if (keep < nin - taken) throw Error(FLN_ERR_INTERNAL, "Barnes-Hut round buffer too small");
-        next += keep;
-      } else {
-        pos += taken - nin;
-      }
-      nin = next;
-      cur = 1 - cur;
-    }
     } catch (...) {
       join();
       throw;
