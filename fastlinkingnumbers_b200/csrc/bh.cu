@@ -2737,6 +2737,26 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaMemcpyAsync(d_segall, seg_all.data(), (nloops + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   TreeArgs T{d_xyz, d_off, d_base, d_loops, nloops, d_children, d_parent, d_leafseg, d_arrive, d_bn, d_hdr, d_mom,
              d_segint};
+  // Slots: pairs ordered by decreasing estimated work. Host work, done once
+  // the tree build is queued (while the GPU runs it, before the host waits
+  // for its counts).
+  std::vector<int32_t> order(np), slot_loops(2 * np);
+  bool slots_ordered = false;
+  auto order_slots = [&]() {
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<double> cost(np);
+    for (int64_t p = 0; p < np; ++p) {
+      const double a = (double)(h_off[h_pairs[2 * p] + 1] - h_off[h_pairs[2 * p]]);
+      const double b = (double)(h_off[h_pairs[2 * p + 1] + 1] - h_off[h_pairs[2 * p + 1]]);
+      cost[p] = (a + b) * std::log2(a + b + 2.0);
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    for (int64_t s = 0; s < np; ++s) {
+      slot_loops[2 * s] = h_pairs[2 * order[s]];
+      slot_loops[2 * s + 1] = h_pairs[2 * order[s] + 1];
+    }
+    slots_ordered = true;
+  };
   int launches = 0;
   FLN_CUDA(cudaEventRecord(ctx.ev2, st));
   if (prm.bh_tree == 1) {
@@ -2835,6 +2855,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
       }
       k0 = k1;
     }
+    order_slots();
     // The device's height counts against the host's, which sized the launches.
     std::vector<int32_t> dev_counts((size_t)64 * group_end.size());
     FLN_CUDA(cudaMemcpyAsync(dev_counts.data(), d_hcnt, dev_counts.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -2848,21 +2869,7 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
   FLN_CUDA(cudaEventRecord(ctx.ev3, st));
   ctx.stats.ms_tree_build = ctx.elapsed(ctx.ev2, ctx.ev3);
 
-  // Slots: pairs ordered by decreasing estimated work.
-  std::vector<int32_t> order(np);
-  std::iota(order.begin(), order.end(), 0);
-  std::vector<double> cost(np);
-  for (int64_t p = 0; p < np; ++p) {
-    const double a = (double)(h_off[h_pairs[2 * p] + 1] - h_off[h_pairs[2 * p]]);
-    const double b = (double)(h_off[h_pairs[2 * p + 1] + 1] - h_off[h_pairs[2 * p + 1]]);
-    cost[p] = (a + b) * std::log2(a + b + 2.0);
-  }
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-  std::vector<int32_t> slot_loops(2 * np);
-  for (int64_t s = 0; s < np; ++s) {
-    slot_loops[2 * s] = h_pairs[2 * order[s]];
-    slot_loops[2 * s + 1] = h_pairs[2 * order[s] + 1];
-  }
+  if (!slots_ordered) order_slots();
   int32_t *d_slots = ctx.d_bh[11].as<int32_t>(4 * np);
   int32_t *d_slot_pair = d_slots + 2 * np;
   int32_t *d_active = d_slots + 3 * np;
