@@ -3242,6 +3242,11 @@ int barnes_hut_device(Context &ctx, const double *d_xyz, const int64_t *d_off, c
     const int64_t p = order[s];
     const double e = err[p] * prm.error_est_scale;
     err[p] = e;
+    // With a positive target, beta* > beta0 needs e > target: below it
+    // (e / target)^(1/4) <= 1 (pow is monotonic and exact at 1), and NaN
+    // compares false either way. The test spares the host most pow calls
+    // while the GPU waits.
+    if (prm.target_error > 0 && !(e > prm.target_error)) continue;
     const double tb = std::min(std::pow(e / prm.target_error, 0.25) * b0, prm.barnes_hut_beta_limit);
     if (tb > b0) {
       retry_slots.push_back((int32_t)s);
