@@ -1,7 +1,10 @@
-"""bench.py's clock sampler: nvidia-smi runs from before the warm-up steps,
-and only the samples whose timestamps fall inside the timed region are
-reported (all of them when none does). The parser is checked here on lines
-in nvidia-smi's CSV format (timestamp first), without a GPU."""
+"""bench.py's host helpers, without a GPU.
+
+The clock sampler: nvidia-smi runs from before the warm-up steps, and only
+the samples whose timestamps fall inside the timed region are reported (all
+of them when none does); the parser is checked on lines in nvidia-smi's CSV
+format (timestamp first). The certificate writer that the CLI leg compares
+byte for byte: checked against the committed certificates."""
 import datetime
 import importlib.util
 import os
